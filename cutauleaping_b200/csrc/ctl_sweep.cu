@@ -1,0 +1,1224 @@
+// Persistent tau-leaping / SSA sweep for sm_100a.
+//
+// Replaces the reference's host loop (kernel.cu:242-345) and its kernels
+// PreCalculations (2phase_n-tau-leaping.cu:1568-2093), EventualSSASteps
+// (2099-2273), LightweightSSA (2280-2454), setup_random (2974-2988),
+// PrepareVariables (1269-1297) and ParallelVoting (2990-3002) with ONE
+// launch: every group of G lanes owns a shared-memory slot, pulls a
+// simulation from a device work queue (atomic ticket), runs it to the end
+// (leaps, SSA bursts, samples) and pulls the next one.  No host round trip
+// per leap, no per-pass reload of state from global memory.
+//
+// Determinism contract (what makes any launch shape give identical bits):
+//   * every random word comes from Philox4x32-10 with key = seed and counter
+//     (block, tag, step, sim): a draw depends on which simulation, which step
+//     and what it is for, never on which thread computes it;
+//   * every FP64 sum over reactions (A0, the critical sum a0c) is the root of
+//     a fixed binary tree over the reactions padded to P = 2^k leaves, and
+//     the SSA / critical-reaction searches descend that same tree;
+//   * per-species sums (mu, sigma^2, population updates) run over a fixed
+//     entry order by one lane.
+// The CPU oracle (oracle/ctl_oracle.c) implements the same contract.
+//
+// Built with -fmad=false: no implicit FMA contraction; fma() is called
+// explicitly where it is meant.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "ctl_internal.h"
+
+namespace ctl {
+namespace dev {
+
+constexpr uint32_t TAG_SSA = 0x40000000u;   // SSA step: (w0,w1) pick, (w2,w3) waiting time
+constexpr uint32_t TAG_MISC = 0x40000001u;  // leap: (w0,w1) tau2, (w2,w3) critical pick
+constexpr uint32_t MAX_ATTEMPTS = 1024u;    // 10-bit attempt field of the Poisson tag
+constexpr uint32_t PTRS_MAX_TRIALS = 256u;
+
+enum : uint32_t {
+    F_FORCE_SSA = 1u << 0, F_Q1_OFF = 1u << 1, F_Q2_OFF = 1u << 2, F_Q3_OFF = 1u << 3,
+    F_Q4_OFF = 1u << 4, F_Q5_OFF = 1u << 5, F_Q6_OFF = 1u << 6, F_Q9_OFF = 1u << 7, F_Q10_OFF = 1u << 8
+};
+
+__device__ __forceinline__ uint32_t tag_pois(uint32_t attempt, uint32_t pair) {
+    return 0x80000000u | (attempt << 20) | pair;
+}
+
+struct Model {
+    int S, R, P, logP, ns, s_out;
+    const uint32_t* __restrict__ reac_off;
+    const uint32_t* __restrict__ reac_ent;
+    const uint32_t* __restrict__ v_off;  // V or F species-major (quirk Q5)
+    const uint32_t* __restrict__ v_ent;
+    const uint32_t* __restrict__ fs_off;
+    const uint32_t* __restrict__ fs_ent;
+    const uint32_t* __restrict__ fr_off;
+    const uint32_t* __restrict__ fr_ent;
+    const uint32_t* __restrict__ dep_off;
+    const uint32_t* __restrict__ dep_ent;
+    const uint8_t* __restrict__ hor;
+    const uint8_t* __restrict__ hort;
+    const double* __restrict__ tvec;
+    const uint32_t* __restrict__ cs;
+    double tmax;
+};
+
+struct Run {
+    uint64_t seed;
+    float eps;
+    uint32_t nc;
+    double ssa_factor;
+    uint32_t ssa_steps, flags, max_steps, sim_base, n;
+    const int32_t* __restrict__ X0;  // [n][S]
+    const float* __restrict__ c;     // [n][R]
+    uint32_t* __restrict__ out;      // [n][ns][s_out]
+    ctl_sim_info* __restrict__ info; // [n]
+    uint32_t* queue;                 // work-queue ticket
+};
+
+// Shared-memory slot layout.  G == 1: element i of slot j at i*NS + j
+// (consecutive threads hit consecutive banks).  G > 1: slot-contiguous
+// arrays of odd padded length (lanes of one group hit distinct banks).
+struct Layout {
+    uint32_t off_X, off_X1, off_a, off_tree, off_K, off_crit, off_c;
+    uint32_t len_S, len_P, len_C;  // padded lengths (G > 1)
+};
+
+// ---------------------------------------------------------------------------
+// Random numbers and elementary functions (bitwise identical to the oracle)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint4 philox10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int i = 0; i < 10; i++) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint4 draw(uint64_t seed, uint32_t blk, uint32_t tag, uint32_t step,
+                                      uint32_t sim) {
+    return philox10(make_uint4(blk, tag, step, sim), (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+__device__ __forceinline__ double u32d(uint32_t w) { return ((double)w + 0.5) * 0x1p-32; }
+__device__ __forceinline__ double u53(uint32_t wa, uint32_t wb) {
+    uint64_t m = ((uint64_t)wb << 20) | (uint64_t)(wa >> 12);
+    return ((double)m + 0.5) * 0x1p-52;
+}
+
+#define CTL_LN2_HI 0x1.62e42fee00000p-1
+#define CTL_LN2_LO 0x1.a39ef35793c76p-33
+
+// log(x) = e ln2 + 2 atanh(s), s = (m-1)/(m+1), m in (sqrt(1/2), sqrt(2)].
+__device__ double dlog(double x) {
+    if (!(x > 0.0)) return x == 0.0 ? __longlong_as_double(0xfff0000000000000ULL)
+                                     : __longlong_as_double(0x7ff8000000000000ULL);
+    if (x == __longlong_as_double(0x7ff0000000000000ULL)) return x;
+    int eadj = 0;
+    if (x < 0x1p-1022) { x = x * 0x1p54; eadj = -54; }
+    uint64_t b = (uint64_t)__double_as_longlong(x);
+    int e = (int)((b >> 52) & 0x7ff) - 1023 + eadj;
+    double m = __longlong_as_double((long long)((b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL));
+    if (m > 0x1.6a09e667f3bcdp+0) { m = m * 0.5; e = e + 1; }
+    double f = m - 1.0;
+    double s = f / (2.0 + f);
+    double z = s * s;
+    double p = 0x1.8618618618618p-5;
+    p = fma(p, z, 0x1.af286bca1af28p-5);
+    p = fma(p, z, 0x1.e1e1e1e1e1e1ep-5);
+    p = fma(p, z, 0x1.1111111111111p-4);
+    p = fma(p, z, 0x1.3b13b13b13b14p-4);
+    p = fma(p, z, 0x1.745d1745d1746p-4);
+    p = fma(p, z, 0x1.c71c71c71c71cp-4);
+    p = fma(p, z, 0x1.2492492492492p-3);
+    p = fma(p, z, 0x1.999999999999ap-3);
+    p = fma(p, z, 0x1.5555555555555p-2);
+    double r = z * p;
+    double ed = (double)e;
+    double two_s = s + s;
+    return fma(ed, CTL_LN2_HI, two_s + fma(two_s, r, ed * CTL_LN2_LO));
+}
+
+// exp(x): Cody-Waite reduction, degree-14 Taylor polynomial, 2^k scaling.
+__device__ double dexp(double x) {
+    if (x != x) return x;
+    if (x > 709.0) return __longlong_as_double(0x7ff0000000000000ULL);
+    if (x < -745.0) return 0.0;
+    double k = rint(x * 0x1.71547652b82fep+0);
+    double r = fma(-k, CTL_LN2_HI, x);
+    r = fma(-k, CTL_LN2_LO, r);
+    double p = 0x1.93974a8c07c9dp-37;
+    p = fma(p, r, 0x1.6124613a86d09p-33);
+    p = fma(p, r, 0x1.1eed8eff8d898p-29);
+    p = fma(p, r, 0x1.ae64567f544e4p-26);
+    p = fma(p, r, 0x1.27e4fb7789f5cp-22);
+    p = fma(p, r, 0x1.71de3a556c734p-19);
+    p = fma(p, r, 0x1.a01a01a01a01ap-16);
+    p = fma(p, r, 0x1.a01a01a01a01ap-13);
+    p = fma(p, r, 0x1.6c16c16c16c17p-10);
+    p = fma(p, r, 0x1.1111111111111p-7);
+    p = fma(p, r, 0x1.5555555555555p-5);
+    p = fma(p, r, 0x1.5555555555555p-3);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    int ki = (int)k;
+    if (ki < -1000) { p = p * 0x1p-200; ki = ki + 200; }
+    return p * __longlong_as_double((long long)((uint64_t)(ki + 1023) << 52));
+}
+
+__constant__ double c_logfact[16] = {
+    0.0, 0.0, 0x1.62e42fefa39efp-1, 0x1.cab0bfa2a2002p+0, 0x1.96ca77c922cf9p+1,
+    0x1.326643c4479c9p+2, 0x1.a51273acf01cap+2, 0x1.10ce1f32dcc30p+3,
+    0x1.5358e82fcb70dp+3, 0x1.99a8921a7f7cfp+3, 0x1.e357590954d15p+3,
+    0x1.180973f3a8d74p+4, 0x1.3fcba16d50143p+4, 0x1.68d5a9c3b32cep+4,
+    0x1.930f3df162a42p+4, 0x1.be636a63fd346p+4};
+
+// log(k!) : table below 16, Stirling series above.
+__device__ double dlogfact(double k) {
+    if (k < 16.0) return c_logfact[(int)k];
+    double x = k + 1.0;
+    double ix = 1.0 / x;
+    double ix2 = ix * ix;
+    double ser = ix * (0x1.5555555555555p-4 -
+                       ix2 * (0x1.6c16c16c16c17p-9 -
+                              ix2 * (0x1.a01a01a01a01ap-11 - ix2 * 0x1.3813813813814p-11)));
+    return (x - 0.5) * dlog(x) - x + 0x1.d67f1c864beb5p-1 + ser;
+}
+
+__device__ __forceinline__ uint32_t clamp_k(double k) {
+    return k > 2147483647.0 ? 2147483647u : (uint32_t)k;
+}
+
+// Poisson(lam) given the reaction's primary uniform pair (wa, wb).
+// lam < 10: sequential inversion.  lam >= 10: Hormann's PTRS (1993); extra
+// trials read blocks 1 + 2j + odd of the same (tag, step, sim) stream.
+__device__ uint32_t poisson(double lam, uint32_t wa, uint32_t wb, uint64_t seed, uint32_t tag,
+                            uint32_t step, uint32_t sim, uint32_t odd) {
+    if (!(lam > 0.0)) return 0u;
+    if (lam < 10.0) {
+        double u = u32d(wa);
+        double p = dexp(-lam);
+        double F = p;
+        uint32_t k = 0;
+        while (u > F && k < 64u) {
+            k = k + 1u;
+            p = (p * lam) / (double)k;
+            F = F + p;
+        }
+        return k;
+    }
+    double slam = sqrt(lam);
+    double loglam = dlog(lam);
+    double b = 0.931 + 2.53 * slam;
+    double a = -0.059 + 0.02483 * b;
+    double invalpha = 1.1239 + 1.1328 / (b - 3.4);
+    double vr = 0.9277 - 3.6224 / (b - 2.0);
+    uint4 w = make_uint4(0u, 0u, 0u, 0u);
+    for (uint32_t t = 0; t < PTRS_MAX_TRIALS; t++) {
+        if (t > 0) {
+            uint32_t j = (t - 1) >> 1;
+            if (((t - 1) & 1u) == 0u) w = draw(seed, 1u + 2u * j + odd, tag, step, sim);
+            wa = ((t - 1) & 1u) ? w.z : w.x;
+            wb = ((t - 1) & 1u) ? w.w : w.y;
+        }
+        double U = u32d(wa) - 0.5;
+        double V = u32d(wb);
+        double us = 0.5 - fabs(U);
+        double k = floor((2.0 * a / us + b) * U + lam + 0.43);
+        if (us >= 0.07 && V <= vr) return clamp_k(k);
+        if (k < 0.0 || (us < 0.013 && V > us)) continue;
+        double lhs = dlog(V) + dlog(invalpha) - dlog(a / (us * us) + b);
+        double rhs = -lam + k * loglam - dlogfact(k);
+        if (lhs <= rhs) return clamp_k(k);
+    }
+    return clamp_k(floor(lam));
+}
+
+// ---------------------------------------------------------------------------
+// Groups and slots
+// ---------------------------------------------------------------------------
+
+template <int G>
+struct Grp {
+    uint32_t lane, mask;
+    __device__ Grp() {
+        lane = threadIdx.x % G;
+        const uint32_t l = threadIdx.x & 31u;
+        mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (l & ~(uint32_t)(G - 1)));
+    }
+    __device__ __forceinline__ void sync() const {
+        if (G > 1) __syncwarp(mask);
+    }
+    __device__ __forceinline__ bool any(bool p) const {
+        if (G == 1) return p;
+        return __any_sync(mask, p) != 0;
+    }
+    __device__ __forceinline__ float fmin(float v) const {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) {
+            float t = __shfl_xor_sync(mask, v, o);
+            v = t < v ? t : v;
+        }
+        return v;
+    }
+    __device__ __forceinline__ unsigned long long sum(unsigned long long v) const {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+        return v;
+    }
+    __device__ __forceinline__ uint32_t bcast(uint32_t v) const {
+        if (G == 1) return v;
+        return __shfl_sync(mask, v, 0, G);
+    }
+};
+
+struct Slot {
+    int32_t* X;
+    int32_t* X1;
+    float* a;
+    double* tree;
+    uint32_t* K;
+    uint8_t* crit;
+    float* c;
+    int st;
+    __device__ __forceinline__ int32_t& x(int i) const { return X[i * st]; }
+    __device__ __forceinline__ int32_t& x1(int i) const { return X1[i * st]; }
+    __device__ __forceinline__ float& pa(int i) const { return a[i * st]; }
+    __device__ __forceinline__ double& t(int i) const { return tree[i * st]; }
+    __device__ __forceinline__ uint32_t& k(int i) const { return K[i * st]; }
+    __device__ __forceinline__ uint8_t& cr(int i) const { return crit[i * st]; }
+    __device__ __forceinline__ float& cf(int i) const { return c[i * st]; }
+};
+
+// Mass-action propensity in FP32 (CalculatePropensity, tau.cu:1443-1470).
+__device__ __forceinline__ float prop(const Model& m, const Slot& sl, int r) {
+    float v = sl.cf(r);
+    const uint32_t e1 = m.reac_off[r + 1];
+    for (uint32_t e = m.reac_off[r]; e < e1; e++) {
+        const uint32_t ent = m.reac_ent[e];
+        const int32_t x = sl.x((int)(ent >> 8));
+        const int st = (int)(ent & 0xffu);
+        if (x < st) return 0.0f;
+        if (st == 1) {
+            v = v * (float)x;
+        } else if (st == 2) {
+            float hx = (float)x;
+            v = v * ((0.5f * hx) * (hx - 1.0f));
+        } else {
+            for (int j = 1; j <= st; j++) v = v * ((float)(x - j + 1) / (float)j);
+        }
+    }
+    return v;
+}
+
+// Cao's g_i (tau.cu:1741-1789) in FP32.
+__device__ __forceinline__ float gfun(uint32_t hor, uint32_t hort, int32_t x) {
+    float xf = (float)x;
+    switch (hor) {
+        case 1: return 1.0f;
+        case 2: return hort == 2 ? 2.0f + 1.0f / (xf - 1.0f) : 2.0f;
+        case 3:
+            if (hort == 3) return 3.0f + 1.0f / (xf - 1.0f) + 2.0f / (xf - 2.0f);
+            if (hort == 2) return 3.0f + 1.5f / (xf - 1.0f);
+            return 3.0f;
+        default: return 1.0f;
+    }
+}
+
+// Tree leaves: mode 0 = propensity, 1 = propensity of critical reactions,
+// 2 = as 1 but leaf 0 unmasked (the reference's critical pick, tau.cu:1997).
+__device__ __forceinline__ double leafv(const Slot& sl, int r, int mode) {
+    float v = sl.pa(r);
+    if (mode == 0) return (double)v;
+    bool on = sl.cr(r) != 0 || (mode == 2 && r == 0);
+    return on ? (double)v : 0.0;
+}
+__device__ __forceinline__ double nodev(const Slot& sl, int i, int P, int mode) {
+    return i < P ? sl.t(i) : leafv(sl, i - P, mode);
+}
+
+template <int G>
+__device__ void build_tree(const Grp<G>& g, const Slot& sl, int P, int mode) {
+    for (int half = P >> 1; half >= 1; half >>= 1) {
+        for (int i = half + (int)g.lane; i < 2 * half; i += G)
+            sl.t(i) = nodev(sl, 2 * i, P, mode) + nodev(sl, 2 * i + 1, P, mode);
+        g.sync();
+    }
+}
+
+// Leftmost leaf whose cumulative weight reaches x; never a zero leaf.
+__device__ __forceinline__ int descend(const Slot& sl, int P, double x, int mode) {
+    int node = 1;
+    while (node < P) {
+        int l = 2 * node;
+        double L = nodev(sl, l, P, mode), Rv = nodev(sl, l + 1, P, mode);
+        if ((x <= L && L > 0.0) || Rv == 0.0) {
+            node = l;
+        } else {
+            x = x - L;
+            node = l + 1;
+        }
+    }
+    return node - P;
+}
+
+template <int G>
+__device__ __forceinline__ void all_props(const Grp<G>& g, const Model& m, const Slot& sl) {
+    for (int r = (int)g.lane; r < m.R; r += G) sl.pa(r) = prop(m, sl, r);
+    g.sync();
+    build_tree<G>(g, sl, m.P, 0);
+}
+
+// After firing r: new propensities for the reactions that depend on the
+// changed species, then their tree paths (or a full rebuild when cheaper);
+// both give the same tree.
+template <int G>
+__device__ void update_after_fire(const Grp<G>& g, const Model& m, const Slot& sl, int r) {
+    const uint32_t d0 = m.dep_off[r], d1 = m.dep_off[r + 1];
+    const uint32_t nd = d1 - d0;
+    if (nd == 0) return;
+    for (uint32_t j = d0 + g.lane; j < d1; j += G) {
+        int rr = (int)m.dep_ent[j];
+        sl.pa(rr) = prop(m, sl, rr);
+    }
+    g.sync();
+    const int P = m.P;
+    if (nd * (uint32_t)m.logP >= (uint32_t)P) {
+        build_tree<G>(g, sl, P, 0);
+        return;
+    }
+    for (int lev = 1; lev <= m.logP; lev++) {
+        for (uint32_t j = d0 + g.lane; j < d1; j += G) {
+            int node = (P + (int)m.dep_ent[j]) >> lev;
+            sl.t(node) = nodev(sl, 2 * node, P, 0) + nodev(sl, 2 * node + 1, P, 0);
+        }
+        g.sync();
+    }
+}
+
+// A0 == 0 (tau.cu:1665-1697, 2165-2196): the reference copies the last
+// recorded sample forward (writing the current state first if none exists).
+template <int G>
+__device__ void finish_zero(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl,
+                            uint32_t* out, uint32_t& cursor) {
+    const int so = m.s_out;
+    const uint32_t ns = (uint32_t)m.ns;
+    if (!(run.flags & F_Q10_OFF)) {
+        if (cursor == 0) {
+            for (int k = (int)g.lane; k < so; k += G) out[k] = (uint32_t)sl.x((int)m.cs[k]);
+            cursor = 1;
+        }
+        for (uint32_t i = cursor; i < ns; i++)
+            for (int k = (int)g.lane; k < so; k += G) out[(size_t)i * so + k] = out[(size_t)(cursor - 1) * so + k];
+    } else {
+        for (uint32_t i = cursor; i < ns; i++)
+            for (int k = (int)g.lane; k < so; k += G) out[(size_t)i * so + k] = (uint32_t)sl.x((int)m.cs[k]);
+    }
+    cursor = ns;
+}
+
+// ---------------------------------------------------------------------------
+// One simulation, start to end, by one group
+// ---------------------------------------------------------------------------
+
+template <int G>
+__device__ void run_sim(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl,
+                        uint32_t sim) {
+    const int S = m.S, R = m.R, P = m.P, so = m.s_out;
+    const uint32_t ns = (uint32_t)m.ns;
+    const uint32_t fl = run.flags;
+    const bool force = (fl & F_FORCE_SSA) != 0;
+    const uint32_t simg = run.sim_base + sim;
+    const uint32_t lane = g.lane;
+    uint32_t* out = run.out + (size_t)sim * ns * (size_t)so;
+
+    g.sync();
+    for (int s = (int)lane; s < S; s += G) sl.x(s) = run.X0[(size_t)sim * S + s];
+    for (int r = (int)lane; r < P; r += G) {
+        sl.cf(r) = r < R ? run.c[(size_t)sim * R + r] : 0.0f;
+        sl.pa(r) = 0.0f;
+        sl.cr(r) = 0;
+    }
+    g.sync();
+    all_props<G>(g, m, sl);
+
+    double T = 0.0, tl = 0.0;
+    uint32_t cursor = 0, n = 0, burst = 0, status = CTL_SIM_OK;
+    uint32_t leaps = 0, ssa = 0, rej = 0;
+    unsigned long long fire = 0;  // lane-local share of the firings
+    bool in_ssa = force;
+    double t_next = m.tvec[0];
+
+    for (;;) {
+        if (!in_ssa) {
+            // ---------------- PreCalculations: decide, then one leap ----------------
+            if (T >= m.tmax) break;
+            if (n >= run.max_steps) { status = CTL_SIM_STEP_LIMIT; break; }
+            const uint32_t step = n++;
+            const double A0 = sl.t(1);
+            if (A0 == 0.0) {
+                finish_zero<G>(g, m, run, sl, out, cursor);
+                T = m.tmax + (double)0.1f;
+                break;
+            }
+            bool lany = false;
+            for (int r = (int)lane; r < R; r += G) {
+                uint8_t cr = 0;
+                const uint32_t e1 = m.reac_off[r + 1];
+                for (uint32_t e = m.reac_off[r]; e < e1; e++) {
+                    const uint32_t ent = m.reac_ent[e];
+                    const uint32_t q = (uint32_t)sl.x((int)(ent >> 8)) / (ent & 0xffu);
+                    if ((fl & F_Q6_OFF) ? (q < run.nc) : (q > 0u && q < run.nc)) cr = 1;
+                }
+                sl.cr(r) = cr;
+                lany |= cr != 0;
+            }
+            const bool anycrit = g.any(lany);
+            g.sync();
+            float t1 = FLT_MAX;
+            for (int s = (int)lane; s < S; s += G) {
+                const uint32_t e0 = m.v_off[s], e1 = m.v_off[s + 1];
+                if (e0 == e1) continue;
+                float mu = 0.0f, sg = 0.0f;
+                for (uint32_t e = e0; e < e1; e++) {
+                    const uint32_t ent = m.v_ent[e];
+                    const int r = (int)(ent >> 8);
+                    if (sl.cr(r)) continue;
+                    const float fv = (float)(int8_t)(ent & 0xffu);
+                    mu = mu + fv * sl.pa(r);
+                    sg = sg + (fv * fv) * sl.pa(r);
+                }
+                const int32_t xs = sl.x(s);
+                const float gg = gfun(m.hor[s], m.hort[s], xs);
+                const float tmp2 = (run.eps * (float)xs) / gg;
+                const float macs = tmp2 > 1.0f ? tmp2 : 1.0f;
+                const bool use = (fl & F_Q9_OFF) ? (sg != 0.0f) : (mu != 0.0f && sg != 0.0f);
+                if (use) {
+                    const float t3 = mu != 0.0f ? macs / fabsf(mu) : __int_as_float(0x7f800000);
+                    const float t4 = (macs * macs) / sg;
+                    const float tt = t3 < t4 ? t3 : t4;
+                    if (tt < t1) t1 = tt;
+                }
+            }
+            const float tau1 = g.fmin(t1);
+            if ((double)tau1 < run.ssa_factor / A0) {
+                in_ssa = true;
+                burst = 0;
+                tl = 0.0;
+                continue;
+            }
+            double a0c = 0.0;
+            if (anycrit) {
+                build_tree<G>(g, sl, P, 1);
+                a0c = sl.t(1);
+            }
+            const uint4 wd = draw(run.seed, 0u, TAG_MISC, step, simg);
+            double tau2 = (double)FLT_MAX;
+            if (a0c > 0.0) tau2 = -dlog(u53(wd.x, wd.y)) / a0c;
+            double tau = (double)tau1 < tau2 ? (double)tau1 : tau2;
+            int pick = -1;
+            if ((double)tau1 > tau2) {
+                int mode = 1;
+                if (!(fl & F_Q2_OFF) && !sl.cr(0)) {
+                    mode = 2;
+                    if (lane == 0)
+                        for (int i = P >> 1; i >= 1; i >>= 1) sl.t(i) = nodev(sl, 2 * i, P, 2) + nodev(sl, 2 * i + 1, P, 2);
+                    g.sync();
+                }
+                pick = descend(sl, P, u53(wd.z, wd.w) * a0c, mode);
+            }
+            uint32_t attempt = 0;
+            bool ovf = false;
+            for (;;) {
+                const bool keep = attempt == 0 || (fl & F_Q3_OFF);
+                for (uint32_t pb = lane; 2u * pb < (uint32_t)R; pb += G) {
+                    const int r0 = (int)(2u * pb), r1 = r0 + 1;
+                    const bool c0 = sl.cr(r0) != 0;
+                    const bool c1 = r1 < R ? sl.cr(r1) != 0 : true;
+                    const double l0 = c0 ? 0.0 : tau * (double)sl.pa(r0);
+                    const double l1 = (c1 || r1 >= R) ? 0.0 : tau * (double)sl.pa(r1);
+                    const uint32_t tg = tag_pois(attempt, pb);
+                    uint4 w = make_uint4(0u, 0u, 0u, 0u);
+                    if (l0 > 0.0 || l1 > 0.0) w = draw(run.seed, 0u, tg, step, simg);
+                    sl.k(r0) = c0 ? ((r0 == pick && keep) ? 1u : 0u)
+                                  : poisson(l0, w.x, w.y, run.seed, tg, step, simg, 0u);
+                    if (r1 < R)
+                        sl.k(r1) = c1 ? ((r1 == pick && keep) ? 1u : 0u)
+                                      : poisson(l1, w.z, w.w, run.seed, tg, step, simg, 1u);
+                }
+                g.sync();
+                bool lfail = false, lovf = false;
+                for (int s = (int)lane; s < S; s += G) {
+                    int64_t x1 = sl.x(s);
+                    const uint32_t e1 = m.fs_off[s + 1];
+                    for (uint32_t e = m.fs_off[s]; e < e1; e++) {
+                        const uint32_t ent = m.fs_ent[e];
+                        x1 += (int64_t)(int8_t)(ent & 0xffu) * (int64_t)sl.k((int)(ent >> 8));
+                        if (!(fl & F_Q4_OFF) && x1 < 0) { lfail = true; break; }
+                    }
+                    if (x1 < 0) lfail = true;
+                    if (x1 > 2147483647LL) lovf = true;
+                    sl.x1(s) = (int32_t)x1;
+                }
+                const bool fail = g.any(lfail);
+                g.sync();
+                if (!fail) {
+                    ovf = g.any(lovf);
+                    break;
+                }
+                tau = tau * 0.5;
+                attempt++;
+                rej++;
+                if (attempt >= MAX_ATTEMPTS) { status = CTL_SIM_ATTEMPT_LIMIT; break; }
+            }
+            if (status != CTL_SIM_OK) break;
+            if (ovf) { status = CTL_SIM_OVERFLOW; break; }
+            // check_time_instant (tau.cu:1507-1562)
+            while (cursor < ns && T + tau >= t_next) {
+                for (int k = (int)lane; k < so; k += G) {
+                    const int s = (int)m.cs[k];
+                    const int32_t xs = sl.x(s);
+                    const double d = (double)((int64_t)sl.x1(s) - (int64_t)xs);
+                    const double delta = (d * (t_next - T)) / tau;
+                    const double ri = rint(delta);
+                    uint32_t v;
+                    if (!(fl & F_Q1_OFF))
+                        v = (uint32_t)xs + (ri > 0.0 ? (uint32_t)ri : 0u);
+                    else
+                        v = (uint32_t)((int64_t)xs + (int64_t)ri);
+                    out[(size_t)cursor * so + k] = v;
+                }
+                cursor++;
+                t_next = cursor < ns ? m.tvec[cursor] : 0.0;
+            }
+            unsigned long long fs = 0;
+            for (int r = (int)lane; r < R; r += G) fs += sl.k(r);
+            fire += fs;
+            leaps++;
+            g.sync();
+            for (int s = (int)lane; s < S; s += G) sl.x(s) = sl.x1(s);
+            g.sync();
+            T = T + tau;
+            all_props<G>(g, m, sl);
+            if (cursor == ns) break;
+        } else {
+            // ---------------- EventualSSASteps / LightweightSSA: one step ----------------
+            if (n >= run.max_steps) { status = CTL_SIM_STEP_LIMIT; break; }
+            const double A0 = sl.t(1);
+            if (A0 == 0.0) {
+                finish_zero<G>(g, m, run, sl, out, cursor);
+                T = m.tmax + (double)0.1f;
+                break;
+            }
+            const uint32_t step = n++;
+            const uint4 wd = draw(run.seed, 0u, TAG_SSA, step, simg);
+            const int r = descend(sl, P, u53(wd.x, wd.y) * A0, 0);
+            const double dt = -dlog(u53(wd.z, wd.w)) / A0;
+            tl = tl + dt;
+            while (cursor < ns && T + tl > t_next) {
+                for (int k = (int)lane; k < so; k += G) out[(size_t)cursor * so + k] = (uint32_t)sl.x((int)m.cs[k]);
+                cursor++;
+                t_next = cursor < ns ? m.tvec[cursor] : 0.0;
+            }
+            g.sync();
+            bool lovf = false;
+            const uint32_t e1 = m.fr_off[r + 1];
+            for (uint32_t e = m.fr_off[r] + lane; e < e1; e += G) {
+                const uint32_t ent = m.fr_ent[e];
+                const int s = (int)(ent >> 8);
+                const int64_t nx = (int64_t)sl.x(s) + (int64_t)(int8_t)(ent & 0xffu);
+                if (nx > 2147483647LL || nx < 0) lovf = true;
+                sl.x(s) = (int32_t)nx;
+            }
+            const bool ovf = g.any(lovf);
+            ssa++;
+            if (lane == 0) fire += 1ull;
+            if (ovf) { status = CTL_SIM_OVERFLOW; break; }
+            g.sync();
+            update_after_fire<G>(g, m, sl, r);
+            burst++;
+            if (cursor == ns) break;
+            if (burst == run.ssa_steps) {
+                T = T + tl;
+                tl = 0.0;
+                burst = 0;
+                if (!force) in_ssa = false;
+                else if (T >= m.tmax) break;
+            }
+        }
+    }
+    for (uint32_t i = cursor; i < ns; i++)
+        for (int k = (int)lane; k < so; k += G) out[(size_t)i * so + k] = 0u;
+    const unsigned long long ftot = g.sum(fire);
+    if (lane == 0) {
+        ctl_sim_info inf;
+        inf.t_final = T + tl;
+        inf.firings = ftot;
+        inf.status = status;
+        inf.steps = n;
+        inf.leaps = leaps;
+        inf.ssa_steps = ssa;
+        inf.rejections = rej;
+        inf.pad = 0;
+        run.info[sim] = inf;
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) sweep_kernel(Model m, Run run, Layout lay) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int NS = (int)(blockDim.x / G);
+    const int j = (int)(threadIdx.x / G);
+    Grp<G> g;
+    Slot sl;
+    if (G == 1) {
+        sl.st = NS;
+        sl.X = reinterpret_cast<int32_t*>(smem + lay.off_X) + j;
+        sl.X1 = reinterpret_cast<int32_t*>(smem + lay.off_X1) + j;
+        sl.a = reinterpret_cast<float*>(smem + lay.off_a) + j;
+        sl.tree = reinterpret_cast<double*>(smem + lay.off_tree) + j;
+        sl.K = reinterpret_cast<uint32_t*>(smem + lay.off_K) + j;
+        sl.crit = reinterpret_cast<uint8_t*>(smem + lay.off_crit) + j;
+        sl.c = reinterpret_cast<float*>(smem + lay.off_c) + j;
+    } else {
+        sl.st = 1;
+        sl.X = reinterpret_cast<int32_t*>(smem + lay.off_X) + (size_t)j * lay.len_S;
+        sl.X1 = reinterpret_cast<int32_t*>(smem + lay.off_X1) + (size_t)j * lay.len_S;
+        sl.a = reinterpret_cast<float*>(smem + lay.off_a) + (size_t)j * lay.len_P;
+        sl.tree = reinterpret_cast<double*>(smem + lay.off_tree) + (size_t)j * lay.len_P;
+        sl.K = reinterpret_cast<uint32_t*>(smem + lay.off_K) + (size_t)j * lay.len_P;
+        sl.crit = reinterpret_cast<uint8_t*>(smem + lay.off_crit) + (size_t)j * lay.len_C;
+        sl.c = reinterpret_cast<float*>(smem + lay.off_c) + (size_t)j * lay.len_P;
+    }
+    for (;;) {
+        uint32_t sim = 0;
+        if (g.lane == 0) sim = atomicAdd(run.queue, 1u);
+        sim = g.bcast(sim);
+        if (sim >= run.n) break;
+        run_sim<G>(g, m, run, sl, sim);
+    }
+}
+
+// calculateFitness (tau.cu:3324-3408): one thread per parameter set.
+__global__ void fitness_kernel(const uint32_t* __restrict__ samples, const uint32_t* __restrict__ target,
+                               const uint8_t* __restrict__ swarm, double* __restrict__ fitness,
+                               uint32_t threads, uint32_t nsets, uint32_t p_rep, uint32_t ns,
+                               uint32_t so, uint32_t E, uint32_t REP) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= nsets) return;
+    const uint32_t b = tid / threads, t = tid % threads;
+    const uint32_t ex = swarm[tid];
+    float sub = 0.0f;
+    for (uint32_t c = 0; c < ns; c++) {
+        for (uint32_t s = 0; s < so; s++) {
+            double acc = 0.0;
+            for (uint32_t par = 0; par < p_rep; par++) {
+                const size_t gid = (size_t)(b * p_rep + par) * threads + t;
+                acc = acc + (double)samples[(gid * ns + c) * so + s];
+            }
+            acc = acc / (double)p_rep;
+            for (uint32_t e = 0; e < REP; e++) {
+                const int tgt = (int)target[((size_t)(c * E + ex) * REP + e) * so + s];
+                double dist = fabs((double)tgt - acc);
+                if (tgt != 0) dist = dist / (double)tgt;
+                sub = (float)((double)sub + dist);
+            }
+        }
+    }
+    fitness[tid] = ((1.0 / (double)ns) * (1.0 / (double)so)) * (double)sub;
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------------------
+// Host launch side
+// ---------------------------------------------------------------------------
+
+static ctl_status cuda_fail(cudaError_t e, const char* what) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return CTL_ERR_CUDA;
+}
+#define CTL_CUDA(call)                                              \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);         \
+    } while (0)
+
+static size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// Upload the model tables to `device` once; later runs reuse them.
+static ctl_status ensure_device(ctl_model* m, int device, DeviceCopy*& out) {
+    if (device < 0 || device >= 16) {
+        set_error("device ordinal out of range");
+        return CTL_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(m->mu);
+    DeviceCopy& d = m->dev[device];
+    if (d.buf) {
+        out = &d;
+        return CTL_OK;
+    }
+    const HostTables& t = m->t;
+    size_t off = 0;
+    auto place = [&](size_t bytes) {
+        size_t o = off;
+        off = align16(off + bytes);
+        return o;
+    };
+    d.off_reac_off = place(t.reac_off.size() * 4);
+    d.off_reac_ent = place(std::max<size_t>(1, t.reac_ent.size()) * 4);
+    d.off_vs_off = place(t.vs_off.size() * 4);
+    d.off_vs_ent = place(std::max<size_t>(1, t.vs_ent.size()) * 4);
+    d.off_fs_off = place(t.fs_off.size() * 4);
+    d.off_fs_ent = place(std::max<size_t>(1, t.fs_ent.size()) * 4);
+    d.off_fr_off = place(t.fr_off.size() * 4);
+    d.off_fr_ent = place(std::max<size_t>(1, t.fr_ent.size()) * 4);
+    d.off_dep_off = place(t.dep_off.size() * 4);
+    d.off_dep_ent = place(std::max<size_t>(1, t.dep_ent.size()) * 4);
+    d.off_hor = place(t.hor.size());
+    d.off_hort = place(t.hort.size());
+    d.off_tvec = place(t.tvec.size() * 8);
+    d.off_cs = place(t.cs.size() * 4);
+    size_t ctrl_off = place(256);
+    d.bytes = off;
+    std::vector<unsigned char> h(d.bytes, 0);
+    auto put = [&](size_t o, const void* p, size_t bytes) {
+        if (bytes) std::memcpy(h.data() + o, p, bytes);
+    };
+    put(d.off_reac_off, t.reac_off.data(), t.reac_off.size() * 4);
+    put(d.off_reac_ent, t.reac_ent.data(), t.reac_ent.size() * 4);
+    put(d.off_vs_off, t.vs_off.data(), t.vs_off.size() * 4);
+    put(d.off_vs_ent, t.vs_ent.data(), t.vs_ent.size() * 4);
+    put(d.off_fs_off, t.fs_off.data(), t.fs_off.size() * 4);
+    put(d.off_fs_ent, t.fs_ent.data(), t.fs_ent.size() * 4);
+    put(d.off_fr_off, t.fr_off.data(), t.fr_off.size() * 4);
+    put(d.off_fr_ent, t.fr_ent.data(), t.fr_ent.size() * 4);
+    put(d.off_dep_off, t.dep_off.data(), t.dep_off.size() * 4);
+    put(d.off_dep_ent, t.dep_ent.data(), t.dep_ent.size() * 4);
+    put(d.off_hor, t.hor.data(), t.hor.size());
+    put(d.off_hort, t.hort.data(), t.hort.size());
+    put(d.off_tvec, t.tvec.data(), t.tvec.size() * 8);
+    put(d.off_cs, t.cs.data(), t.cs.size() * 4);
+    int prev = 0;
+    CTL_CUDA(cudaGetDevice(&prev));
+    CTL_CUDA(cudaSetDevice(device));
+    void* buf = nullptr;
+    cudaError_t e = cudaMalloc(&buf, d.bytes);
+    if (e != cudaSuccess) {
+        cudaSetDevice(prev);
+        set_error(std::string("cudaMalloc(model tables): ") + cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? CTL_ERR_OOM : CTL_ERR_CUDA;
+    }
+    e = cudaMemcpy(buf, h.data(), d.bytes, cudaMemcpyHostToDevice);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        cudaFree(buf);
+        return cuda_fail(e, "cudaMemcpy(model tables)");
+    }
+    d.buf = buf;
+    d.device = device;
+    d.ctrl = reinterpret_cast<uint32_t*>(static_cast<unsigned char*>(buf) + ctrl_off);
+    out = &d;
+    return CTL_OK;
+}
+
+static dev::Model make_dev_model(const ctl_model* m, const DeviceCopy& d, uint32_t flags) {
+    const HostTables& t = m->t;
+    auto P = [&](size_t o) { return static_cast<const unsigned char*>(d.buf) + o; };
+    dev::Model dm;
+    dm.S = t.S; dm.R = t.R; dm.P = t.P; dm.logP = t.logP; dm.ns = t.ns; dm.s_out = t.s_out;
+    dm.reac_off = reinterpret_cast<const uint32_t*>(P(d.off_reac_off));
+    dm.reac_ent = reinterpret_cast<const uint32_t*>(P(d.off_reac_ent));
+    const bool q5off = (flags & dev::F_Q5_OFF) != 0;
+    dm.v_off = reinterpret_cast<const uint32_t*>(P(q5off ? d.off_fs_off : d.off_vs_off));
+    dm.v_ent = reinterpret_cast<const uint32_t*>(P(q5off ? d.off_fs_ent : d.off_vs_ent));
+    dm.fs_off = reinterpret_cast<const uint32_t*>(P(d.off_fs_off));
+    dm.fs_ent = reinterpret_cast<const uint32_t*>(P(d.off_fs_ent));
+    dm.fr_off = reinterpret_cast<const uint32_t*>(P(d.off_fr_off));
+    dm.fr_ent = reinterpret_cast<const uint32_t*>(P(d.off_fr_ent));
+    dm.dep_off = reinterpret_cast<const uint32_t*>(P(d.off_dep_off));
+    dm.dep_ent = reinterpret_cast<const uint32_t*>(P(d.off_dep_ent));
+    dm.hor = P(d.off_hor);
+    dm.hort = P(d.off_hort);
+    dm.tvec = reinterpret_cast<const double*>(P(d.off_tvec));
+    dm.cs = reinterpret_cast<const uint32_t*>(P(d.off_cs));
+    dm.tmax = t.tmax;
+    return dm;
+}
+
+struct LaunchPlan {
+    int G = 1, threads = 256, NS = 256, blocks = 1, blocks_per_sm = 1, sm_count = 1, regs = 0;
+    size_t smem = 0;
+    dev::Layout lay{};
+};
+
+static size_t slot_layout(const HostTables& t, int G, int NS, dev::Layout& lay) {
+    size_t off = 0;
+    auto region = [&](size_t bytes) {
+        size_t o = off;
+        off = align16(off + bytes);
+        return (uint32_t)o;
+    };
+    if (G == 1) {
+        lay.len_S = (uint32_t)t.S;
+        lay.len_P = (uint32_t)t.P;
+        lay.len_C = (uint32_t)t.P;
+    } else {
+        lay.len_S = (uint32_t)(t.S | 1);
+        lay.len_P = (uint32_t)(t.P + 1);
+        lay.len_C = (uint32_t)(((t.P + 3) & ~3) + 4);
+    }
+    lay.off_tree = region((size_t)NS * lay.len_P * 8);
+    lay.off_X = region((size_t)NS * lay.len_S * 4);
+    lay.off_X1 = region((size_t)NS * lay.len_S * 4);
+    lay.off_a = region((size_t)NS * lay.len_P * 4);
+    lay.off_K = region((size_t)NS * lay.len_P * 4);
+    lay.off_c = region((size_t)NS * lay.len_P * 4);
+    lay.off_crit = region((size_t)NS * lay.len_C);
+    return off;
+}
+
+template <int G>
+static const void* kernel_ptr() {
+    return reinterpret_cast<const void*>(&dev::sweep_kernel<G>);
+}
+static const void* kernel_for(int G) {
+    switch (G) {
+        case 1: return kernel_ptr<1>();
+        case 2: return kernel_ptr<2>();
+        case 4: return kernel_ptr<4>();
+        case 8: return kernel_ptr<8>();
+        case 16: return kernel_ptr<16>();
+        case 32: return kernel_ptr<32>();
+    }
+    return nullptr;
+}
+
+static int heuristic_group(const HostTables& t) {
+    int g = t.P / 8;
+    int G = 1;
+    while (G < g && G < 32) G <<= 1;
+    return G;
+}
+
+// Launch shape for (model, cfg, n): group size, threads, slots and grid.
+static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, LaunchPlan& pl) {
+    const HostTables& t = m->t;
+    int G = cfg->group > 0 ? cfg->group : heuristic_group(t);
+    if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32) {
+        set_error("group must be one of 1, 2, 4, 8, 16, 32");
+        return CTL_ERR_ARG;
+    }
+    if (G > t.P) G = t.P;
+    int threads = cfg->threads > 0 ? cfg->threads : 256;
+    if (threads % 32 || threads < 32 || threads > 256) {
+        set_error("threads per block must be a multiple of 32 in [32, 256]");
+        return CTL_ERR_ARG;
+    }
+    int dev_id = cfg->device;
+    cudaDeviceProp prop;
+    CTL_CUDA(cudaGetDeviceProperties(&prop, dev_id));
+    const size_t smem_max = prop.sharedMemPerBlockOptin;
+    for (;;) {
+        int NS = threads / G;
+        size_t bytes = slot_layout(t, G, NS, pl.lay);
+        if (bytes <= smem_max) {
+            pl.smem = bytes;
+            pl.NS = NS;
+            break;
+        }
+        if (threads <= 32) {
+            set_error("network too large: one simulation slot needs " + std::to_string(bytes / NS) +
+                      " bytes of shared memory");
+            return CTL_ERR_SHAPE;
+        }
+        threads -= 32;
+    }
+    pl.G = G;
+    pl.threads = threads;
+    const void* k = kernel_for(G);
+    CTL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
+    int bps = 0;
+    CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, pl.smem));
+    if (bps < 1) {
+        set_error("sweep kernel cannot be resident with this shape");
+        return CTL_ERR_SHAPE;
+    }
+    cudaFuncAttributes fa;
+    CTL_CUDA(cudaFuncGetAttributes(&fa, k));
+    pl.regs = fa.numRegs;
+    pl.blocks_per_sm = bps;
+    pl.sm_count = prop.multiProcessorCount;
+    uint64_t need = (n + (uint64_t)pl.NS - 1) / pl.NS;
+    uint64_t cap = (uint64_t)bps * prop.multiProcessorCount;
+    pl.blocks = (int)std::max<uint64_t>(1, std::min(need, cap));
+    return CTL_OK;
+}
+
+static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* dX0,
+                                const float* dc, uint32_t* dout, ctl_sim_info* dinfo,
+                                cudaStream_t stream, const LaunchPlan& pl, const DeviceCopy& d) {
+    dev::Run run;
+    run.seed = cfg->seed;
+    run.eps = cfg->eps;
+    run.nc = cfg->nc;
+    run.ssa_factor = cfg->ssa_factor;
+    run.ssa_steps = cfg->ssa_steps;
+    run.flags = cfg->flags;
+    run.max_steps = cfg->max_steps;
+    run.sim_base = cfg->sim_base;
+    run.n = n;
+    run.X0 = dX0;
+    run.c = dc;
+    run.out = dout;
+    run.info = dinfo;
+    run.queue = d.ctrl;
+    dev::Model dm = make_dev_model(m, d, cfg->flags);
+    CTL_CUDA(cudaMemsetAsync(d.ctrl, 0, sizeof(uint32_t), stream));
+    void* args[] = {&dm, &run, const_cast<dev::Layout*>(&pl.lay)};
+    CTL_CUDA(cudaLaunchKernel(kernel_for(pl.G), dim3((unsigned)pl.blocks), dim3((unsigned)pl.threads), args,
+                              pl.smem, stream));
+    return CTL_OK;
+}
+
+static ctl_status check_cfg(const ctl_run_cfg* cfg) {
+    if (!cfg) {
+        set_error("null run configuration");
+        return CTL_ERR_ARG;
+    }
+    if (cfg->ssa_steps == 0) {
+        set_error("ssa_steps must be positive");
+        return CTL_ERR_ARG;
+    }
+    return CTL_OK;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        cudaGetDevice(&prev);
+        cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace ctl
+
+using namespace ctl;
+
+struct ctl_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int device = 0;
+};
+
+extern "C" void ctl_model_free(ctl_model* m) {
+    if (!m) return;
+    for (auto& d : m->dev) {
+        if (d.buf) {
+            int prev = 0;
+            cudaGetDevice(&prev);
+            cudaSetDevice(d.device);
+            cudaFree(d.buf);
+            cudaSetDevice(prev);
+            d.buf = nullptr;
+        }
+    }
+    delete m;
+}
+
+extern "C" ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
+                                       ctl_launch_info* li) {
+    if (!m || !li) return CTL_ERR_ARG;
+    ctl_status st = check_cfg(cfg);
+    if (st != CTL_OK) return st;
+    DeviceGuard dg(cfg->device);
+    LaunchPlan pl;
+    st = plan_launch(m, cfg, n, pl);
+    if (st != CTL_OK) return st;
+    li->group = pl.G;
+    li->threads = pl.threads;
+    li->blocks = pl.blocks;
+    li->slots_per_block = pl.NS;
+    li->smem_bytes = (int32_t)pl.smem;
+    li->regs_per_thread = pl.regs;
+    li->blocks_per_sm = pl.blocks_per_sm;
+    li->sm_count = pl.sm_count;
+    return CTL_OK;
+}
+
+extern "C" ctl_status ctl_run_device(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
+                                     const int32_t* d_X0, const float* d_c, uint32_t* d_samples,
+                                     ctl_sim_info* d_info, void* stream) {
+    if (!m) return CTL_ERR_ARG;
+    ctl_status st = check_cfg(cfg);
+    if (st != CTL_OK) return st;
+    if (n == 0) return CTL_OK;
+    if (!d_X0 || !d_c || !d_samples || !d_info) {
+        set_error("null device buffer");
+        return CTL_ERR_ARG;
+    }
+    DeviceGuard dg(cfg->device);
+    DeviceCopy* d = nullptr;
+    if ((st = ensure_device(m, cfg->device, d)) != CTL_OK) return st;
+    LaunchPlan pl;
+    if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;
+    return enqueue_sweep(m, cfg, n, d_X0, d_c, d_samples, d_info, static_cast<cudaStream_t>(stream), pl, *d);
+}
+
+extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* X0,
+                              const float* c, uint32_t* samples, ctl_sim_info* info) {
+    if (!m) return CTL_ERR_ARG;
+    ctl_status st = check_cfg(cfg);
+    if (st != CTL_OK) return st;
+    if (n == 0) return CTL_OK;
+    if (!X0 || !c || !samples || !info) {
+        set_error("null host buffer");
+        return CTL_ERR_ARG;
+    }
+    const HostTables& t = m->t;
+    DeviceGuard dg(cfg->device);
+    DeviceCopy* d = nullptr;
+    if ((st = ensure_device(m, cfg->device, d)) != CTL_OK) return st;
+    LaunchPlan pl;
+    if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;
+    const size_t bx = (size_t)n * t.S * 4, bc = (size_t)n * t.R * 4;
+    const size_t bo = (size_t)n * t.ns * t.s_out * 4, bi = (size_t)n * sizeof(ctl_sim_info);
+    cudaStream_t s;
+    CTL_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    void *dx = nullptr, *dc = nullptr, *dout = nullptr, *dinf = nullptr;
+    cudaError_t e = cudaMallocAsync(&dx, bx, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dc, bc, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dout, bo, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dinf, bi, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dx, X0, bx, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dc, c, bc, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        st = enqueue_sweep(m, cfg, n, static_cast<int32_t*>(dx), static_cast<float*>(dc),
+                           static_cast<uint32_t*>(dout), static_cast<ctl_sim_info*>(dinf), s, pl, *d);
+        if (st != CTL_OK) e = cudaErrorLaunchFailure;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(samples, dout, bo, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(info, dinf, bi, cudaMemcpyDeviceToHost, s);
+    if (dx) cudaFreeAsync(dx, s);
+    if (dc) cudaFreeAsync(dc, s);
+    if (dout) cudaFreeAsync(dout, s);
+    if (dinf) cudaFreeAsync(dinf, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (st != CTL_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "ctl_run");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "ctl_run (sweep)");
+    for (uint32_t i = 0; i < n; i++)
+        if (info[i].status != CTL_SIM_OK) {
+            set_error("simulation " + std::to_string(i) + " ended with status " + std::to_string(info[i].status));
+            return CTL_ERR_STEP_LIMIT;
+        }
+    return CTL_OK;
+}
+
+extern "C" ctl_status ctl_graph_create(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
+                                       const int32_t* d_X0, const float* d_c, uint32_t* d_samples,
+                                       ctl_sim_info* d_info, void* stream, ctl_graph** out) {
+    if (!m || !out) return CTL_ERR_ARG;
+    *out = nullptr;
+    ctl_status st = check_cfg(cfg);
+    if (st != CTL_OK) return st;
+    DeviceGuard dg(cfg->device);
+    DeviceCopy* d = nullptr;
+    if ((st = ensure_device(m, cfg->device, d)) != CTL_OK) return st;
+    LaunchPlan pl;
+    if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStream_t cap = s;
+    bool own = false;
+    if (cap == nullptr) {
+        CTL_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        own = true;
+    }
+    ctl_graph* g = new ctl_graph();
+    g->device = cfg->device;
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        st = enqueue_sweep(m, cfg, n, d_X0, d_c, d_samples, d_info, cap, pl, *d);
+        cudaError_t e2 = cudaStreamEndCapture(cap, &g->graph);
+        if (st == CTL_OK && e2 != cudaSuccess) e = e2;
+    }
+    if (e == cudaSuccess && st == CTL_OK) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    if (own) cudaStreamDestroy(cap);
+    if (e != cudaSuccess || st != CTL_OK) {
+        ctl_graph_free(g);
+        return st != CTL_OK ? st : cuda_fail(e, "ctl_graph_create");
+    }
+    *out = g;
+    return CTL_OK;
+}
+
+extern "C" ctl_status ctl_graph_launch(ctl_graph* g, void* stream) {
+    if (!g || !g->exec) return CTL_ERR_ARG;
+    DeviceGuard dg(g->device);
+    CTL_CUDA(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
+    return CTL_OK;
+}
+
+extern "C" void ctl_graph_free(ctl_graph* g) {
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+}
+
+extern "C" ctl_status ctl_fitness(ctl_model* m, const ctl_target* t, const ctl_run_cfg* cfg,
+                                  const uint32_t* samples, double* fitness) {
+    if (!m || !t || !cfg || !samples || !fitness) return CTL_ERR_ARG;
+    const HostTables& h = m->t;
+    if (t->ns != (uint32_t)h.ns || t->s_out != (uint32_t)h.s_out) {
+        set_error("fitness target does not match the model's samples");
+        return CTL_ERR_SHAPE;
+    }
+    DeviceGuard dg(cfg->device);
+    const uint64_t N = (uint64_t)t->threads * t->blocks;
+    const uint32_t nsets = (uint32_t)(N / t->p_rep);
+    const size_t bs = (size_t)N * h.ns * h.s_out * 4, bt = t->series.size() * 4, bw = (size_t)N;
+    cudaStream_t s;
+    CTL_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    void *ds = nullptr, *dt = nullptr, *dw = nullptr, *df = nullptr;
+    cudaError_t e = cudaMallocAsync(&ds, bs, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dt, std::max<size_t>(bt, 4), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dw, std::max<size_t>(bw, 4), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&df, (size_t)N * 8, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, samples, bs, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && bt) e = cudaMemcpyAsync(dt, t->series.data(), bt, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dw, t->thread2experiment.data(), bw, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(df, 0, (size_t)N * 8, s);
+    if (e == cudaSuccess && nsets) {
+        dev::fitness_kernel<<<(nsets + 127) / 128, 128, 0, s>>>(
+            static_cast<uint32_t*>(ds), static_cast<uint32_t*>(dt), static_cast<uint8_t*>(dw),
+            static_cast<double*>(df), t->threads, nsets, t->p_rep, (uint32_t)h.ns, (uint32_t)h.s_out,
+            t->experiments, t->repetitions);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(fitness, df, (size_t)N * 8, cudaMemcpyDeviceToHost, s);
+    if (ds) cudaFreeAsync(ds, s);
+    if (dt) cudaFreeAsync(dt, s);
+    if (dw) cudaFreeAsync(dw, s);
+    if (df) cudaFreeAsync(df, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess) return cuda_fail(e, "ctl_fitness");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "ctl_fitness (kernel)");
+    return CTL_OK;
+}

@@ -1,0 +1,180 @@
+/*
+ * ctl.h -- C ABI of cutauleaping_b200, a B200-native (sm_100a) drop-in for
+ * the simulation path of aresio/cuTauLeaping.
+ *
+ * The reference has no library API: its boundary is the process command
+ * line (kernel.cu:74-119), the input-folder text format
+ * (2phase_n-tau-leaping.cu:57-1261) and one output file per simulation
+ * (2phase_n-tau-leaping.cu:3431-3507).  This header is the C ABI beneath
+ * that boundary; the `cutauleaping` CLI is a thin wrapper over it, and any
+ * host language binds it through its C FFI.
+ *
+ * Conventions
+ *   - Every entry point returns ctl_status; none calls exit().
+ *   - Host buffers belong to the caller.  Device tables live inside the
+ *     opaque ctl_model and are freed by ctl_model_free().
+ *   - Per-simulation arrays are simulation-major: X0 [n][S], c [n][R],
+ *     samples [n][ns][s_out] (uint32), info [n].
+ *   - Results depend only on (model, rows, seed, sim_base, flags); launch
+ *     shape, grouping and autotuning never change a single bit.
+ *   - One run at a time per (model, device): runs share the model's queue
+ *     counter on that device.
+ */
+#ifndef CTL_H
+#define CTL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    CTL_OK = 0,
+    CTL_ERR_IO = 1,          /* a file could not be opened / read / written        */
+    CTL_ERR_PARSE = 2,       /* malformed number or line in an input file          */
+    CTL_ERR_SHAPE = 3,       /* inconsistent sizes (rows, columns, species ids)    */
+    CTL_ERR_CUDA = 4,        /* CUDA runtime error (message in ctl_last_error())   */
+    CTL_ERR_OOM = 5,         /* host or device allocation failed                    */
+    CTL_ERR_STEP_LIMIT = 6,  /* at least one simulation ended with a non-OK status */
+    CTL_ERR_TIMEOUT = 7,     /* reserved: bounded device waits gave up             */
+    CTL_ERR_ARG = 8          /* invalid argument                                   */
+} ctl_status;
+
+/* Per-simulation status (ctl_sim_info.status). */
+typedef enum {
+    CTL_SIM_OK = 0,
+    CTL_SIM_STEP_LIMIT = 1,     /* step counter reached ctl_run_cfg.max_steps        */
+    CTL_SIM_OVERFLOW = 2,       /* a population exceeded INT32_MAX                   */
+    CTL_SIM_ATTEMPT_LIMIT = 3   /* 1024 consecutive negative-population rejections   */
+} ctl_sim_status;
+
+/* Switches that turn OFF one reference quirk each; 0 reproduces the
+ * reference algorithm (2phase_n-tau-leaping.cu line numbers in brackets). */
+enum {
+    CTL_FORCE_SSA = 1u << 0, /* exact SSA only, LightweightSSA [2280-2454]       */
+    CTL_Q1_OFF = 1u << 1,    /* signed interpolation of samples [1538-1541]      */
+    CTL_Q2_OFF = 1u << 2,    /* mask PROP[0] in the critical pick [1997]         */
+    CTL_Q3_OFF = 1u << 3,    /* keep the critical firing on retry [2044-2046]    */
+    CTL_Q4_OFF = 1u << 4,    /* reject on final negatives only [1327-1329]       */
+    CTL_Q5_OFF = 1u << 5,    /* tau1 over feed-masked F, not V [1860-1922]       */
+    CTL_Q6_OFF = 1u << 6,    /* critical iff floor(X/L) < nc [1731]              */
+    CTL_Q9_OFF = 1u << 7,    /* sigma bound also when mu == 0 [1904-1911]        */
+    CTL_Q10_OFF = 1u << 8    /* A0 == 0 fills with the current state [1665-1697] */
+};
+
+typedef struct ctl_model ctl_model;
+typedef struct ctl_target ctl_target;
+typedef struct ctl_graph ctl_graph;
+
+typedef struct {
+    int32_t S, R, P;            /* species, reactions, tree width (pow2 >= R)   */
+    int32_t ns, s_out;          /* sample instants, sampled species             */
+    int32_t nnz_left, nnz_var, nnz_feared, nnz_dep;
+    double tmax;                /* last sample instant = simulated end time     */
+} ctl_model_dims;
+
+typedef struct {
+    uint64_t seed;        /* Philox key; the reference used time(NULL) (kernel.cu:176) */
+    float eps;            /* Cao epsilon, 0.03 (2phase_n-tau-leaping.cuh:76)           */
+    uint32_t nc;          /* critical threshold, 10 (2phase_n-tau-leaping.cuh:75)      */
+    double ssa_factor;    /* SSA hand-off when tau1 < ssa_factor/A0, 10 (tau.cu:1935)  */
+    uint32_t ssa_steps;   /* SSA burst length, 100 (kernel.cu:83)                      */
+    uint32_t flags;       /* CTL_FORCE_SSA | CTL_Q*_OFF                                */
+    uint32_t max_steps;   /* per-simulation step cap (CTL_SIM_STEP_LIMIT)              */
+    uint32_t sim_base;    /* global index of row 0 (the reference's `offset`)          */
+    int32_t device;       /* CUDA device ordinal                                       */
+    int32_t group;        /* lanes per simulation: 1,2,4,8,16,32; 0 = autotune         */
+    int32_t threads;      /* threads per block; 0 = autotune                           */
+    int32_t reserved;
+} ctl_run_cfg;
+
+typedef struct {
+    double t_final;
+    uint64_t firings;     /* sum of K over accepted leaps + executed SSA steps */
+    uint32_t status;      /* ctl_sim_status                                    */
+    uint32_t steps, leaps, ssa_steps, rejections, pad;
+} ctl_sim_info;
+
+typedef struct {
+    int32_t group, threads, blocks, slots_per_block;
+    int32_t smem_bytes, regs_per_thread, blocks_per_sm, sm_count;
+} ctl_launch_info;
+
+/* ---- errors ------------------------------------------------------------ */
+const char* ctl_status_str(ctl_status s);
+/* Message of the last failure on the calling thread ("" if none). */
+const char* ctl_last_error(void);
+
+/* ---- models -------------------------------------------------------------- */
+/* Replaces first_pass + read_stoichiometry + read_instants
+ * (tau.cu:90-120, 122-457, 932-1053): reads left_side, right_side, M_feed
+ * (optional), t_vector and cs_vector (optional) from `folder`. */
+ctl_status ctl_model_load(const char* folder, ctl_model** out);
+/* Same model from dense arrays: left/right [R][S], feed [S] or NULL,
+ * tvec [ns], cs [s_out] or NULL (all species). */
+ctl_status ctl_model_create(int32_t S, int32_t R, const int32_t* left, const int32_t* right,
+                            const int32_t* feed, int32_t ns, const double* tvec,
+                            int32_t s_out, const int32_t* cs, ctl_model** out);
+void ctl_model_free(ctl_model* m);
+ctl_status ctl_model_dims_get(const ctl_model* m, ctl_model_dims* dims);
+/* HOR / HORtype per species (tau.cu:402-432). */
+ctl_status ctl_model_hor(const ctl_model* m, uint8_t* hor, uint8_t* hort);
+
+/* Replaces read_quantities_offset + read_parameters_offset (tau.cu:570-649,
+ * 717-782): rows [offset, offset+n) of MX_0 and c_matrix.  X0 [n][S] and
+ * c [n][R] are caller buffers (rate constants stored FP32). */
+ctl_status ctl_rows_load(const char* folder, int32_t S, int32_t R, uint32_t offset,
+                         uint32_t n, int32_t* X0, float* c);
+
+/* ---- simulation ---------------------------------------------------------- */
+void ctl_run_cfg_default(ctl_run_cfg* cfg);
+/* Replaces the host loop kernel.cu:155-345 (setup_random, PrepareVariables,
+ * PreCalculations / EventualSSASteps / LightweightSSA, ParallelVoting) with
+ * one persistent sweep.  Host buffers in and out; copies are inside the call.
+ * Returns CTL_ERR_STEP_LIMIT if any simulation ended with a non-OK status. */
+ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* X0,
+                   const float* c, uint32_t* samples, ctl_sim_info* info);
+/* The same sweep on device buffers, enqueued on `stream` (cudaStream_t). */
+ctl_status ctl_run_device(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
+                          const int32_t* d_X0, const float* d_c, uint32_t* d_samples,
+                          ctl_sim_info* d_info, void* stream);
+/* Launch shape the sweep would use (after autotuning when cfg asks for it). */
+ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
+                            ctl_launch_info* li);
+
+/* One CUDA graph holding the whole sweep (queue reset + persistent kernel);
+ * replay with ctl_graph_launch.  Buffers are bound at creation. */
+ctl_status ctl_graph_create(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
+                            const int32_t* d_X0, const float* d_c, uint32_t* d_samples,
+                            ctl_sim_info* d_info, void* stream, ctl_graph** out);
+ctl_status ctl_graph_launch(ctl_graph* g, void* stream);
+void ctl_graph_free(ctl_graph* g);
+
+/* ---- output -------------------------------------------------------------- */
+/* WriteDynamics2 (tau.cu:3431-3469): file <path_prefix>_<first_id + i> per
+ * simulation, rows "t<TAB>x..." with iostream default formatting. */
+ctl_status ctl_write_dynamics(const ctl_model* m, const char* path_prefix, uint32_t n,
+                              const uint32_t* samples, uint32_t first_id, int32_t nthreads);
+/* PrintDynamics2 (tau.cu:3472-3507): the same rows to stdout, a blank line
+ * after each simulation. */
+ctl_status ctl_print_dynamics(const ctl_model* m, uint32_t n, const uint32_t* samples);
+
+/* ---- fitness ------------------------------------------------------------- */
+/* read_time_series (tau.cu:1056-1261): ts_rep, p_rep, ts_numtgt, tts_vector,
+ * ts_matrix for a run of threads*blocks simulations. */
+ctl_status ctl_target_load(const char* folder, const ctl_model* m, uint32_t threads,
+                           uint32_t blocks, ctl_target** out);
+void ctl_target_free(ctl_target* t);
+ctl_status ctl_target_dims(const ctl_target* t, uint32_t* repetitions, uint32_t* p_rep,
+                           uint32_t* target_quantities, uint32_t* experiments);
+/* calculateFitness (tau.cu:3324-3408) on the GPU: fitness [threads*blocks]
+ * (entries past threads*blocks/p_rep are 0). */
+ctl_status ctl_fitness(ctl_model* m, const ctl_target* t, const ctl_run_cfg* cfg,
+                       const uint32_t* samples, double* fitness);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,116 @@
+"""Generate statistical golden fixtures from the reference binary itself.
+
+The reference (aresio/cuTauLeaping) ships no tests, golden outputs or example
+inputs, and seeds cuRAND from time(NULL) (kernel.cu:176), so its output can
+only be pinned statistically.  This script runs the reference binary built
+from its own sources (oracle/_ref/cuTauLeaping, see oracle/Makefile) on
+seeded input folders written by cutauleaping_b200.inputs, parses the dynamics
+it prints (PrintDynamics2, 2phase_n-tau-leaping.cu:3472-3507, selected with
+verbose = 2) and stores per-sample means and variances plus the raw values at
+a few sample instants, so that tests can compare the CPU oracle against the
+reference's own trajectories (3-standard-error and two-sample KS checks).
+
+Run on a machine with a GPU (the reference has no CPU path):
+    python tests/golden/make_reference_fixtures.py --out tests/golden
+"""
+import argparse
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from cutauleaping_b200 import inputs  # noqa: E402
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "cuTauLeaping")
+
+def _syn12x20():
+    """12 species / 20 reactions (generator seed 0), with reaction 0 replaced
+    by a zero-order inflow ->X0 at rate 1.  The reference's critical-reaction
+    search (2phase_n-tau-leaping.cu:1993-2006) starts from PROP[0] and can walk
+    past the last reaction when PROP[0] == 0 and the FP32-rounded target
+    exceeds the critical sum; a positive zero-order reaction 0 keeps every
+    read of that loop in bounds."""
+    net = inputs.synthetic(12, 20, 4096, seed=0, t_end=2.0, samples=50, x0_range=(20, 2000))
+    net.left[0] = 0
+    net.right[0] = 0
+    net.right[0, 0] = 1
+    net.c[:, 0] = 1.0
+    return net
+
+
+# name -> (network factory, threads, blocks, force_ssa, species columns kept raw)
+CASES = {
+    "schlogl": (lambda: inputs.schlogl(4096), 64, 64, False, [1]),
+    "schlogl_ssa": (lambda: inputs.schlogl(4096), 64, 64, True, [1]),
+    "syn12x20": (_syn12x20, 32, 128, False, list(range(12))),
+}
+RAW_EVERY = 10  # keep raw values at every 10th sample instant
+
+
+def parse_print_dynamics(text: str, n: int, ns: int, so: int) -> np.ndarray:
+    """Rows `t<TAB>x...` per simulation, a blank line after each (PrintDynamics2)."""
+    out = np.zeros((n, ns, so), dtype=np.uint32)
+    sim, row = 0, 0
+    for line in text.splitlines():
+        if not line.strip():
+            if row:
+                if row != ns:
+                    raise ValueError(f"simulation {sim}: {row} rows, expected {ns}")
+                sim, row = sim + 1, 0
+            continue
+        if line.startswith(" *") or line.startswith("T=") or line.startswith("WARNING"):
+            continue
+        parts = line.split("\t")
+        if len(parts) != so + 1:
+            continue
+        out[sim, row] = [int(v) for v in parts[1:]]
+        row += 1
+    if sim != n:
+        raise ValueError(f"parsed {sim} simulations, expected {n}")
+    return out
+
+
+def run_case(name, factory, threads, blocks, force, keep, outdir):
+    net = factory()
+    n = threads * blocks
+    assert net.n == n
+    with tempfile.TemporaryDirectory() as td:
+        folder = inputs.write_folder(os.path.join(td, name), net)
+        args = [REF_BIN, folder, str(threads), str(blocks), "0", "0", os.path.join(td, "out"),
+                "pref", "0", "1" if force else "0", "2"]
+        t0 = time.time()
+        p = subprocess.run(args, capture_output=True, text=True, timeout=900)
+        wall = time.time() - t0
+        if p.returncode != 0:
+            raise RuntimeError(f"{name}: reference exited {p.returncode}: {p.stderr[-2000:]}")
+    so = net.S if net.cs is None else len(net.cs)
+    samples = parse_print_dynamics(p.stdout, n, len(net.tvec), so)
+    x = samples.astype(np.float64)
+    raw_idx = np.arange(RAW_EVERY - 1, len(net.tvec), RAW_EVERY)
+    path = os.path.join(outdir, f"reference_{name}.npz")
+    np.savez_compressed(
+        path, mean=x.mean(axis=0), var=x.var(axis=0, ddof=1), n=n, tvec=net.tvec,
+        raw_idx=raw_idx, raw=samples[:, raw_idx][:, :, keep].astype(np.uint32), raw_species=keep,
+        force_ssa=force, wall_s=wall, threads=threads, blocks=blocks)
+    print(f"{name}: {n} simulations, reference wall {wall:.2f}s -> {path}", flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    ap.add_argument("--cases", nargs="*", default=list(CASES))
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    if not os.path.exists(REF_BIN):
+        sys.exit(f"{REF_BIN} missing: build it with `make -C oracle ref` where the reference sources exist")
+    for name in a.cases:
+        run_case(name, *CASES[name], a.out)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,77 @@
+"""GPU parity: the CUDA sweep reproduces the CPU oracle bit for bit.
+
+Every test calls the product through its C ABI (libctl.so via ctypes) and
+compares against oracle/ (the C restatement of PreCalculations,
+EventualSSASteps and LightweightSSA, 2phase_n-tau-leaping.cu:1568-2454) on the
+same seeded inputs.  Samples and per-simulation counters are integers and are
+compared exactly; t_final is an FP64 value produced by the same sequence of
+IEEE operations and is compared exactly as well.
+"""
+import numpy as np
+import pytest
+
+import cutauleaping_b200 as ctl
+from tests.netutil import oracle_run, same_info, small_networks
+
+pytestmark = pytest.mark.gpu
+
+NETS = small_networks()
+
+
+def gpu_run(net, **kw):
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    return m.run(net.X0, net.c, **kw)
+
+
+@pytest.mark.parametrize("name,net", NETS, ids=[n for n, _ in NETS])
+def test_bit_exact_vs_oracle(name, net):
+    out_o, info_o = oracle_run(net, seed=123)
+    out_g, info_g = gpu_run(net, seed=123)
+    assert np.array_equal(out_g, out_o), f"{name}: samples differ"
+    assert same_info(info_g, info_o) is None, f"{name}: info field {same_info(info_g, info_o)} differs"
+    assert (info_g["status"] == ctl.SIM_OK).all()
+
+
+@pytest.mark.parametrize("flags", [ctl.FORCE_SSA, ctl.Q1_OFF, ctl.Q2_OFF, ctl.Q3_OFF, ctl.Q4_OFF,
+                                   ctl.Q5_OFF, ctl.Q6_OFF, ctl.Q9_OFF, ctl.Q10_OFF,
+                                   ctl.ALL_QUIRKS_OFF, ctl.ALL_QUIRKS_OFF | ctl.FORCE_SSA])
+def test_quirk_switches_bit_exact(flags):
+    for name, net in NETS[:4]:
+        out_o, info_o = oracle_run(net, seed=7, flags=flags)
+        out_g, info_g = gpu_run(net, seed=7, flags=flags)
+        assert np.array_equal(out_g, out_o), f"{name} flags={flags:#x}"
+        assert same_info(info_g, info_o) is None, f"{name} flags={flags:#x}"
+
+
+@pytest.mark.parametrize("name,net", NETS, ids=[n for n, _ in NETS])
+def test_launch_shape_invariance(name, net):
+    ref, ref_info = gpu_run(net, seed=99, group=1, threads=256)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    for G in (1, 2, 4, 8, 16, 32):
+        for threads in (32, 96, 256):
+            if threads % G:
+                continue
+            out, info = m.run(net.X0, net.c, seed=99, group=G, threads=threads)
+            assert np.array_equal(out, ref), f"{name} G={G} threads={threads}"
+            assert same_info(info, ref_info) is None, f"{name} G={G} threads={threads}"
+
+
+def test_sim_base_selects_rows_of_a_larger_run():
+    """The reference's `offset` shards rows; with sim_base the shard reproduces
+    the same simulations a single large run produces."""
+    name, net = NETS[1]
+    full, _ = gpu_run(net, seed=5)
+    part, _ = gpu_run(net.subset(slice(10, 30)), seed=5, sim_base=10)
+    assert np.array_equal(part, full[10:30])
+
+
+def test_step_limit_status_without_hang():
+    name, net = NETS[0]
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    out, info = m.run(net.X0, net.c, seed=1, max_steps=50, check=False)
+    assert (info["status"] == ctl.SIM_STEP_LIMIT).all()
+    assert (info["steps"] == 50).all()
+    out_o, info_o = oracle_run(net, seed=1, max_steps=50)
+    assert np.array_equal(out, out_o)
+    with pytest.raises(ctl.CtlError):
+        m.run(net.X0, net.c, seed=1, max_steps=50)

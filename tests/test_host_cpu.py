@@ -1,0 +1,161 @@
+"""Host logic of the product on CPU: the C ABI loads and exports every symbol
+include/ctl.h declares, the input-folder parsers (2phase_n-tau-leaping.cu
+first_pass 90-120, read_stoichiometry 122-457, read_quantities_offset 570-649,
+read_parameters_offset 717-782, read_instants 932-1053) produce the same
+tables as the oracle, their error paths return statuses instead of exiting,
+the dynamics writer is byte-compatible with WriteDynamics2 (3431-3469), and
+the CLI's early exits keep the reference's exit codes.  No GPU calls."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import cutauleaping_b200 as ctl
+import oracle
+from cutauleaping_b200 import inputs
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol():
+    hdr = open(os.path.join(ROOT, "include", "ctl.h")).read()
+    declared = set(re.findall(r"\b(ctl_[a-z_]+)\s*\(", hdr))
+    assert declared == set(ctl.EXPORTS)
+    L = ctl.lib()
+    for name in declared:
+        assert hasattr(L, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", ctl.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r" T (ctl_\w+)", out))
+    assert declared <= exported
+
+
+def test_schlogl_folder_roundtrip(tmp_path):
+    net = inputs.schlogl(32)
+    folder = inputs.write_folder(str(tmp_path / "schlogl"), net)
+    m = ctl.Model.load(folder)
+    assert (m.S, m.R, m.P, m.ns, m.s_out) == (3, 4, 4, 100, 3)
+    assert m.tmax == 5.0
+    X0, c = ctl.load_rows(folder, m, 0, 32)
+    assert np.array_equal(X0, net.X0)
+    assert np.array_equal(c, net.c.astype(np.float32))
+    X0b, _ = ctl.load_rows(folder, m, 5, 3)
+    assert np.array_equal(X0b, net.X0[5:8])
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_hor_tables_match_oracle(seed):
+    left, right, _, _ = inputs.random_network(10, 24, seed, max_order=3)
+    tvec = np.linspace(0.1, 1, 10)
+    m = ctl.Model.create(left, right, None, tvec)
+    om = oracle.OracleModel(left, right, None, tvec)
+    h1, t1 = m.hor()
+    h2, t2 = om.hor()
+    assert np.array_equal(h1, h2) and np.array_equal(t1, t2)
+
+
+def test_schlogl_hor_is_the_reference_value():
+    net = inputs.schlogl(1)
+    hor, hort = ctl.Model.create(net.left, net.right, net.feed, net.tvec).hor()
+    # A: order-3 reaction with coefficient 1; X: order 3, max coefficient 3; B: order 1.
+    assert list(hor) == [3, 3, 1] and list(hort) == [1, 3, 1]
+
+
+def _folder(tmp_path, **edits):
+    net = inputs.schlogl(8)
+    folder = inputs.write_folder(str(tmp_path / "m"), net)
+    for name, text in edits.items():
+        path = os.path.join(folder, name)
+        if text is None:
+            os.remove(path)
+        else:
+            with open(path, "w") as f:
+                f.write(text)
+    return folder
+
+
+@pytest.mark.parametrize("edit,status", [
+    ({"left_side": None}, ctl.ERR_IO),
+    ({"t_vector": None}, ctl.ERR_IO),
+    ({"left_side": "1\t2\t0\n0\t3\n0\t0\t1\n0\t1\t0\n"}, ctl.ERR_SHAPE),
+    ({"right_side": "0\t3\t0\n1\t2\t0\n"}, ctl.ERR_SHAPE),
+    ({"left_side": "1\tx\t0\n0\t3\t0\n0\t0\t1\n0\t1\t0\n"}, ctl.ERR_PARSE),
+    ({"left_side": "-1\t2\t0\n0\t3\t0\n0\t0\t1\n0\t1\t0\n"}, ctl.ERR_SHAPE),
+    ({"cs_vector": "0\n7\n"}, ctl.ERR_SHAPE),
+])
+def test_model_load_errors(tmp_path, edit, status):
+    folder = _folder(tmp_path, **edit)
+    with pytest.raises(ctl.CtlError) as e:
+        ctl.Model.load(folder)
+    assert e.value.status == status
+
+
+def test_missing_optional_files(tmp_path):
+    folder = _folder(tmp_path, M_feed=None, cs_vector=None)
+    m = ctl.Model.load(folder)
+    assert m.s_out == 3
+
+
+@pytest.mark.parametrize("edit,n,status", [
+    ({}, 9, ctl.ERR_SHAPE),                                        # read_quantities_offset exit(-4)
+    ({"MX_0": "1\t2\n" * 8}, 8, ctl.ERR_SHAPE),                    # exit(-5)
+    ({"MX_0": None}, 8, ctl.ERR_IO),                               # exit(-6)
+    ({"c_matrix": "1\t2\t3\n" * 8}, 8, ctl.ERR_SHAPE),             # too many / few parameters
+    ({"c_matrix": "1\t2\t3\t4\n" * 4}, 8, ctl.ERR_SHAPE),          # fewer rows than requested
+    ({"MX_0": "1\t-2\t3\n" * 8}, 8, ctl.ERR_SHAPE),                # negative population
+])
+def test_rows_load_errors(tmp_path, edit, n, status):
+    folder = _folder(tmp_path, **edit)
+    m = ctl.Model.create(*[np.array(x) for x in ([[1, 2, 0], [0, 3, 0], [0, 0, 1], [0, 1, 0]],
+                                                  [[0, 3, 0], [1, 2, 0], [0, 1, 0], [0, 0, 1]])],
+                         [1, 0, 1], np.arange(1, 11) * 0.5)
+    with pytest.raises(ctl.CtlError) as e:
+        ctl.load_rows(folder, m, 0, n)
+    assert e.value.status == status
+
+
+def test_write_dynamics_format(tmp_path):
+    net = inputs.schlogl(3, samples=7, t_end=1e-4 * 7)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    rng = np.random.default_rng(0)
+    samples = rng.integers(0, 2**32 - 1, size=(3, 7, 3), dtype=np.uint64).astype(np.uint32)
+    prefix = str(tmp_path / "pref")
+    m.write_dynamics(prefix, samples, threads=2)
+    for gid in range(3):
+        got = open(f"{prefix}_{gid}").read()
+        # std::ostream default formatting of a double == printf("%g")
+        exp = "".join("%g" % t + "".join(f"\t{v}" for v in samples[gid, i]) + "\n"
+                      for i, t in enumerate(net.tvec))
+        assert got == exp
+
+
+def test_fitness_target_load(tmp_path):
+    net = inputs.schlogl(8, samples=5, t_end=1.0)
+    ts = np.arange(5 * 2 * 3 * 3).reshape(5, 2, 3, 3)
+    target = {"ts_rep": 3, "p_rep": 2, "ts_numtgt": 3, "tts_vector": [4, 8], "ts_matrix": ts}
+    folder = inputs.write_folder(str(tmp_path / "f"), net, target)
+    m = ctl.Model.load(folder)
+    t = ctl.Target(folder, m, threads=2, blocks=4)
+    assert (t.repetitions, t.p_rep, t.target_quantities, t.experiments) == (3, 2, 3, 2)
+    with pytest.raises(ctl.CtlError):
+        ctl.Target(folder, m, threads=2, blocks=3)   # p_rep does not divide blocks
+
+
+def _cli(*args, cwd=None):
+    return subprocess.run([ctl.CLI_PATH, *map(str, args)], capture_output=True, text=True,
+                          cwd=cwd, timeout=60)
+
+
+def test_cli_usage_and_early_exit_codes(tmp_path):
+    p = _cli("only", "three", "args")
+    assert p.returncode == 255 and "ERROR: please specify" in p.stdout
+    folder = _folder(tmp_path)
+    p = _cli(folder, 4, 4, 0, 0, tmp_path / "out", "pref", 0, 0, 0)     # 16 rows > 8 in MX_0
+    assert p.returncode == 256 - 4, p.stderr
+    p = _cli(tmp_path / "nope", 2, 2, 0, 0, tmp_path / "out", "pref", 0, 0, 0)
+    assert p.returncode == 255
+    folder2 = _folder(tmp_path / "x", MX_0=None)
+    p = _cli(folder2, 2, 2, 0, 0, tmp_path / "out", "pref", 0, 0, 0)
+    assert p.returncode == 256 - 6
