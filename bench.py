@@ -1,0 +1,343 @@
+"""Benchmark: simulations/s (and reaction firings/s) of the tau-leaping sweep.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--config 2]
+
+Workload (default): the synthetic mass-action network of configs[1] -- 64
+species, 128 reactions of order 0-2 (generator seed 0), rate constants
+log-uniform in [1e-4, 1], initial counts log-uniform in [10, 1e4] -- for
+65,536 simulations per GPU, t_end = 10, 200 samples, eps = 0.03.  One step =
+one complete sweep (every simulation from t = 0 to t_end), launched as one
+CUDA graph (work-queue reset + persistent kernel).
+
+  value     sims/s with inputs resident in HBM, CUDA-event time per step on the
+            launching stream, L2 flushed (256 MB write) between steps, max over
+            ranks.
+  e2e       the same metric through the C ABI call a user makes (ctl_run) with
+            pinned host buffers: H2D of X0/c, the sweep, D2H of all samples and
+            per-simulation records, timed on the host around the call.
+  --impl reference
+            the reference routine on the host cores: the C restatement in
+            oracle/ (the reference has no CPU implementation of its own), all
+            host threads, a bounded sample of the same workload per step.
+
+Multi-GPU (torchrun): every rank simulates its own 65,536 simulations
+(disjoint Philox streams via sim_base), no collective on the data path;
+value = all simulations / max-over-ranks time ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sims/sec & reaction firings/sec on 1 B200 vs host build; surrogate-screened fits/sec"
+
+
+def workload(config: int, n: int | None = None):
+    from cutauleaping_b200 import inputs
+    if config == 1:
+        net = inputs.schlogl(n or 4096)
+        desc = (f"Schlogl bistable model (schlogl.xml), {net.n} simulations, t_end=5, "
+                f"100 samples, eps=0.03, SSA factor 10, n_c=10")
+    else:
+        net = inputs.synthetic(64, 128, n or 65536, seed=0, t_end=10.0, samples=200)
+        desc = (f"synthetic mass-action network 64 species x 128 reactions (order 0-2, generator "
+                f"seed 0), {net.n} simulations, t_end=10, 200 samples, eps=0.03")
+    return net, desc
+
+
+def op_count(net, info):
+    """Algorithmic 32-bit-op count of the sweep under a fixed convention:
+    SSA step 6R + 2 nnz_F/R + 60; leap attempt 44R + 4 nnz_V + 8S + 2 nnz_F + 60;
+    SSA hand-off decision 4R + 4 nnz_V + 8S."""
+    S, R = net.S, net.R
+    V = net.right - net.left
+    F = V * (1 - net.feed[None, :])
+    nnz_v, nnz_f = int((V != 0).sum()), int((F != 0).sum())
+    w_ssa = 6 * R + 2 * nnz_f / R + 60
+    w_leap = 44 * R + 4 * nnz_v + 8 * S + 2 * nnz_f + 60
+    w_hand = 4 * R + 4 * nnz_v + 8 * S
+    ssa = info["ssa_steps"].astype(np.float64)
+    att = info["leaps"].astype(np.float64) + info["rejections"]
+    hand = np.maximum(info["steps"].astype(np.float64) - ssa - info["leaps"], 0)
+    return float((ssa * w_ssa + att * w_leap + hand * w_hand).sum())
+
+
+def algorithmic_bytes(net):
+    """HBM bytes one simulation must move: X0 (4S) + c (4R) + samples
+    (4 ns s_out) + its 40-byte record."""
+    so = net.S if net.cs is None else len(net.cs)
+    return 4 * net.S + 4 * net.R + 4 * len(net.tvec) * so + 40
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def cpu_reference(net, desc, steps, warmup, sample_s=10.0, threads=None):
+    """The reference routine on the host: oracle port, all host threads,
+    bounded samples of the same workload.  Returns (sims/s, firings/s, meta)."""
+    import oracle
+    threads = threads or os.cpu_count() or 1
+    m = oracle.OracleModel(net.left, net.right, net.feed, net.tvec, net.cs, seed=1)
+    c32 = net.c.astype(np.float32)
+    # size the sample so that one step takes about `sample_s` seconds
+    k = min(net.n, max(threads, 64))
+    t0 = time.perf_counter()
+    m.run(net.X0[:k], c32[:k], threads=threads)
+    per = (time.perf_counter() - t0) / k
+    k = int(min(net.n, max(threads, sample_s / max(per, 1e-9))))
+    vals, fvals = [], []
+    for i in range(warmup + steps):
+        lo = (i * k) % max(1, net.n - k + 1)
+        t0 = time.perf_counter()
+        _, info = m.run(net.X0[lo:lo + k], c32[lo:lo + k], sim_base=lo, threads=threads)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            vals.append(k / dt)
+            fvals.append(float(info["firings"].sum()) / dt)
+    return float(np.mean(vals)), float(np.mean(fvals)), {
+        "cores": threads, "sample": f"{k} of the {net.n} simulations per step ({desc.split(',')[0]})"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2])
+    ap.add_argument("--sims", type=int, default=None, help="simulations per GPU (default: config's)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    net, desc = workload(a.config, a.sims)
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        v, fv, meta = cpu_reference(net, desc, a.steps, a.warmup)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "sims/s",
+            "firings_per_s": fv, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32/f64/i32", "data": "synthetic",
+            "config": {"workload": desc, "sims": net.n},
+            "cpu_baseline": {"value": v, "unit": "sims/s", "cores": meta["cores"], "kind": "port",
+                             "sample": meta["sample"]},
+            "e2e": {"value": v, "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+        return
+
+    import torch
+    import cutauleaping_b200 as ctl
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    n = net.n
+    sim_base = rank * n
+    cfg = ctl.run_cfg(seed=1, sim_base=sim_base, device=local)
+    li = model.launch_info(n, cfg)
+    dev = torch.device("cuda", local)
+    X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).to(dev)
+    c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).to(dev)
+    out = torch.empty((n, model.ns, model.s_out), dtype=torch.int32, device=dev)
+    info = torch.empty((n, 40), dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    graph = model.graph(n, X0.data_ptr(), c.data_ptr(), out.data_ptr(), info.data_ptr(),
+                        stream.cuda_stream, cfg)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    with torch.cuda.stream(stream):
+        for _ in range(a.warmup):
+            flush.fill_(1)
+            graph.launch(stream.cuda_stream)
+        stream.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(a.steps)]
+        barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            for e0, e1 in ev:
+                flush.fill_(1)
+                e0.record(stream)
+                graph.launch(stream.cuda_stream)
+                e1.record(stream)
+            stream.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+    times = [e0.elapsed_time(e1) for e0, e1 in ev]
+    ms = float(np.mean(times))
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    inf = info.cpu().numpy().view(ctl.INFO_DTYPE).reshape(-1)
+    fire = float(inf["firings"].sum())
+    if dist is not None:
+        f = torch.tensor([fire], dtype=torch.float64, device=dev)
+        dist.all_reduce(f)
+        fire = float(f.item())
+    value = world * n / (ms * 1e-3)
+    ops = op_count(net, inf)
+    abytes = algorithmic_bytes(net) * n
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    issue_peak = li.sm_count * 128 * sm_mhz * 1e6  # FP32/INT32 lanes per SM x clock
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("bytes_per_launch")
+        except (OSError, ValueError):
+            traffic = None
+
+    e2e = None
+    if not a.no_e2e:
+        hX0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).pin_memory()
+        hc = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).pin_memory()
+        hout = torch.empty((n, model.ns, model.s_out), dtype=torch.int32).pin_memory()
+        hinfo = torch.empty((n, 40), dtype=torch.uint8).pin_memory()
+        import ctypes as C
+        L = ctl.lib()
+
+        def call():
+            st = L.ctl_run(model.handle, C.byref(cfg), n, C.c_void_p(hX0.data_ptr()),
+                           C.c_void_p(hc.data_ptr()), C.c_void_p(hout.data_ptr()),
+                           C.c_void_p(hinfo.data_ptr()))
+            if st not in (ctl.OK, ctl.ERR_STEP_LIMIT):
+                raise ctl.CtlError(st, "ctl_run")
+        call()
+        barrier()
+        et = []
+        for _ in range(max(1, min(a.steps, 3))):
+            t0 = time.perf_counter()
+            call()
+            et.append(time.perf_counter() - t0)
+        e2e_s = float(np.mean(et))
+        if dist is not None:
+            t = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * n / e2e_s, "unit": "sims/s",
+               "h2d_bytes_per_step": int(hX0.numel() * 4 + hc.numel() * 4),
+               "d2h_bytes_per_step": int(hout.numel() * 4 + hinfo.numel()),
+               "ms_per_step": e2e_s * 1e3, "timer": "host perf_counter around ctl_run"}
+        same = bool(np.array_equal(hout.numpy(), out.cpu().numpy()))
+        e2e["bit_identical_to_device_run"] = same
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        v, fv, meta = cpu_reference(net, desc, 1, 0)
+        cpu = {"value": v, "unit": "sims/s", "cores": meta["cores"], "kind": "port",
+               "sample": meta["sample"], "firings_per_s": fv}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "sims/s",
+            "firings_per_s": fire / (ms * 1e-3),
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64/i32", "data": "synthetic",
+            "config": {"workload": desc, "sims_per_gpu": n, "seed": 1,
+                       "l2": "flushed between steps by a 256 MB device write",
+                       "launch": {"group": li.group, "threads": li.threads, "blocks": li.blocks,
+                                  "slots_per_block": li.slots_per_block, "smem_bytes": li.smem_bytes,
+                                  "regs": li.regs_per_thread, "blocks_per_sm": li.blocks_per_sm},
+                       "parallelism": f"dp{world} (independent simulations per rank)"},
+            "roofline": {"bound": "hbm", "achieved": abytes / (ms * 1e-3) / 1e9,
+                         "peak": hbm_peak, "unit": "GB/s",
+                         "frac": abytes / (ms * 1e-3) / 1e9 / hbm_peak,
+                         "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
+                         "note": "HBM is not the bound of this issue-bound kernel; see roofline_issue"},
+            "roofline_issue": {"achieved": ops / (ms * 1e-3) / 1e12, "peak": issue_peak / 1e12,
+                               "unit": "Tops/s", "frac": ops / (ms * 1e-3) / issue_peak,
+                               "convention": "32-bit ops per SSA step / leap attempt (bench.op_count)",
+                               "peak_source": f"{li.sm_count} SMs x 128 FP32/INT32 lanes x median SM clock"},
+            "gpu_launches": a.steps,
+            "clocks": clocks,
+            "per_sim": {"steps": float(inf["steps"].mean()), "leaps": float(inf["leaps"].mean()),
+                        "ssa_steps": float(inf["ssa_steps"].mean()),
+                        "status_ok": int((inf["status"] == 0).sum())},
+        }
+        if e2e is not None:
+            line["e2e"] = e2e
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    del graph
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
