@@ -195,7 +195,8 @@ def main():
     model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
     n = net.n
     sim_base = rank * n
-    cfg = ctl.run_cfg(seed=1, sim_base=sim_base, device=local)
+    cfg = ctl.run_cfg(seed=1, sim_base=sim_base, device=local,
+                      uniform_rates=int(bool((net.c == net.c[0]).all())))
     li = model.launch_info(n, cfg)
     dev = torch.device("cuda", local)
     X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).to(dev)
@@ -254,11 +255,12 @@ def main():
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "sweep_traffic.json")
-    if os.path.exists(tf):
+    tf = os.path.join(ROOT, "profiles", "sweep_traffic.txt")
+    if os.path.exists(tf) and a.config == 2 and n == 65536:
         try:
-            traffic = json.load(open(tf)).get("bytes_per_launch")
-        except (OSError, ValueError):
+            line = open(tf).read().split("#")[0]
+            traffic = float(line.split(":")[1]) / 1e9  # GB per launch
+        except (OSError, ValueError, IndexError):
             traffic = None
 
     e2e = None
@@ -317,7 +319,9 @@ def main():
             "roofline": {"bound": "hbm", "achieved": abytes / (ms * 1e-3) / 1e9,
                          "peak": hbm_peak, "unit": "GB/s",
                          "frac": abytes / (ms * 1e-3) / 1e9 / hbm_peak,
-                         "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
+                         "traffic": traffic, "traffic_unit": "GB per launch (ncu, scaled)",
+                         "algorithmic_gb_per_launch": abytes / 1e9,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
                          "note": "HBM is not the bound of this issue-bound kernel; see roofline_issue"},
             "roofline_issue": {"achieved": ops / (ms * 1e-3) / 1e12, "peak": issue_peak / 1e12,
                                "unit": "Tops/s", "frac": ops / (ms * 1e-3) / issue_peak,

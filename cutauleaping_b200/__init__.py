@@ -49,7 +49,8 @@ class RunCfg(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("eps", C.c_float), ("nc", C.c_uint32),
                 ("ssa_factor", C.c_double), ("ssa_steps", C.c_uint32), ("flags", C.c_uint32),
                 ("max_steps", C.c_uint32), ("sim_base", C.c_uint32), ("device", C.c_int32),
-                ("group", C.c_int32), ("threads", C.c_int32), ("reserved", C.c_int32)]
+                ("group", C.c_int32), ("threads", C.c_int32), ("uniform_rates", C.c_int32),
+                ("ssa_budget", C.c_int32), ("dec_budget", C.c_int32), ("reserved", C.c_int32)]
 
 
 class ModelDims(C.Structure):
@@ -127,12 +128,14 @@ def _check(status: int, where: str):
 
 
 def run_cfg(*, seed=0, eps=0.03, nc=10, ssa_factor=10.0, ssa_steps=100, flags=0,
-            max_steps=0xFFFFFFFF, sim_base=0, device=0, group=0, threads=0) -> RunCfg:
+            max_steps=0xFFFFFFFF, sim_base=0, device=0, group=0, threads=0, uniform_rates=0,
+            ssa_budget=0, dec_budget=0) -> RunCfg:
     cfg = RunCfg()
     lib().ctl_run_cfg_default(C.byref(cfg))
     cfg.seed, cfg.eps, cfg.nc, cfg.ssa_factor = seed, eps, nc, ssa_factor
     cfg.ssa_steps, cfg.flags, cfg.max_steps, cfg.sim_base = ssa_steps, flags, max_steps, sim_base
     cfg.device, cfg.group, cfg.threads = device, group, threads
+    cfg.uniform_rates, cfg.ssa_budget, cfg.dec_budget = uniform_rates, ssa_budget, dec_budget
     return cfg
 
 

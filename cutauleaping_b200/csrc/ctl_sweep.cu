@@ -35,7 +35,7 @@
 namespace ctl {
 namespace dev {
 
-constexpr uint32_t TAG_SSA = 0x40000000u;   // SSA step: (w0,w1) pick, (w2,w3) waiting time
+constexpr uint32_t TAG_SSA = 0x40000000u;   // SSA steps 2b, 2b+1: block b, (w0,w1) / (w2,w3)
 constexpr uint32_t TAG_MISC = 0x40000001u;  // leap: (w0,w1) tau2, (w2,w3) critical pick
 constexpr uint32_t MAX_ATTEMPTS = 1024u;    // 10-bit attempt field of the Poisson tag
 constexpr uint32_t PTRS_MAX_TRIALS = 256u;
@@ -66,6 +66,12 @@ struct Model {
     const double* __restrict__ tvec;
     const uint32_t* __restrict__ cs;
     double tmax;
+    // Stored levels of the binary sum tree: level 3, 6, 9, ... below the
+    // root, and the root.  Stored level li holds the nodes that cover 2^shift
+    // leaves; each is the pairwise sum of 2^d nodes of stored level li-1
+    // (li = 0: of leaves).  Intermediate levels are recomputed in registers.
+    int nlev;
+    int lev_shift[10], lev_d[10], lev_base[10], lev_count[10];
 };
 
 struct Run {
@@ -74,6 +80,8 @@ struct Run {
     uint32_t nc;
     double ssa_factor;
     uint32_t ssa_steps, flags, max_steps, sim_base, n;
+    uint32_t uniform_c;              // all simulations share row 0 of c
+    uint32_t ssa_budget, dec_budget; // work per slot and round (SSA steps / decisions)
     const int32_t* __restrict__ X0;  // [n][S]
     const float* __restrict__ c;     // [n][R]
     uint32_t* __restrict__ out;      // [n][ns][s_out]
@@ -85,9 +93,18 @@ struct Run {
 // (consecutive threads hit consecutive banks).  G > 1: slot-contiguous
 // arrays of odd padded length (lanes of one group hit distinct banks).
 struct Layout {
-    uint32_t off_X, off_X1, off_a, off_tree, off_K, off_crit, off_c;
-    uint32_t len_S, len_P, len_C;  // padded lengths (G > 1)
+    uint32_t off_X, off_X1, off_a, off_K, off_tree, off_crit, off_c, off_state, off_list;
+    uint32_t len_S, len_P, len_C, len_T;  // padded lengths (G > 1)
 };
+
+// Per-slot scalars, one array each (index = slot).
+struct StateArrays {
+    double *T, *tl, *tnext;
+    unsigned long long* fire;
+    uint32_t *sim, *cursor, *n, *burst, *leaps, *ssa, *rej, *flags;
+};
+constexpr uint32_t ST_IN_SSA = 1u, ST_STATUS_SHIFT = 8;
+constexpr uint32_t PH_EMPTY = 0u, PH_DECIDE = 1u, PH_SSA = 2u, PH_CLOSED = 3u;
 
 // ---------------------------------------------------------------------------
 // Random numbers and elementary functions (bitwise identical to the oracle)
@@ -176,6 +193,28 @@ __device__ double dexp(double x) {
     if (ki < -1000) { p = p * 0x1p-200; ki = ki + 200; }
     return p * __longlong_as_double((long long)((uint64_t)(ki + 1023) << 52));
 }
+
+// FP32 log(x) for normal x > 0: the reduction of dlog in single precision,
+// series 2s(1 + s^2/3 + s^4/5 + s^6/7 + s^8/9).
+__device__ __forceinline__ float flog(float x) {
+    const uint32_t b = __float_as_uint(x);
+    int e = (int)((b >> 23) & 0xffu) - 127;
+    float m = __uint_as_float((b & 0x007fffffu) | 0x3f800000u);
+    if (m > 0x1.6a09e6p+0f) { m = m * 0.5f; e = e + 1; }
+    const float f = m - 1.0f;
+    const float sv = f / (2.0f + f);
+    const float z = sv * sv;
+    float p = 0x1.c71c72p-4f;
+    p = fmaf(p, z, 0x1.24924ap-3f);
+    p = fmaf(p, z, 0x1.99999ap-3f);
+    p = fmaf(p, z, 0x1.555556p-2f);
+    const float r = z * p;
+    const float ef = (float)e;
+    const float two_s = sv + sv;
+    return fmaf(ef, 0x1.62e4p-1f, two_s + fmaf(two_s, r, ef * 0x1.7f7d1cp-20f));
+}
+
+__device__ __forceinline__ float u24f(uint32_t w) { return ((float)(w >> 8) + 0.5f) * 0x1p-24f; }
 
 __constant__ double c_logfact[16] = {
     0.0, 0.0, 0x1.62e42fefa39efp-1, 0x1.cab0bfa2a2002p+0, 0x1.96ca77c922cf9p+1,
@@ -291,14 +330,15 @@ struct Slot {
     uint32_t* K;
     uint8_t* crit;
     float* c;
-    int st;
+    int st;   // element stride of the slot arrays
+    int cst;  // element stride of the rate constants (1 when shared by the block)
     __device__ __forceinline__ int32_t& x(int i) const { return X[i * st]; }
     __device__ __forceinline__ int32_t& x1(int i) const { return X1[i * st]; }
     __device__ __forceinline__ float& pa(int i) const { return a[i * st]; }
     __device__ __forceinline__ double& t(int i) const { return tree[i * st]; }
     __device__ __forceinline__ uint32_t& k(int i) const { return K[i * st]; }
     __device__ __forceinline__ uint8_t& cr(int i) const { return crit[i * st]; }
-    __device__ __forceinline__ float& cf(int i) const { return c[i * st]; }
+    __device__ __forceinline__ float& cf(int i) const { return c[i * cst]; }
 };
 
 // Mass-action propensity in FP32 (CalculatePropensity, tau.cu:1443-1470).
@@ -344,40 +384,84 @@ __device__ __forceinline__ double leafv(const Slot& sl, int r, int mode) {
     bool on = sl.cr(r) != 0 || (mode == 2 && r == 0);
     return on ? (double)v : 0.0;
 }
-__device__ __forceinline__ double nodev(const Slot& sl, int i, int P, int mode) {
-    return i < P ? sl.t(i) : leafv(sl, i - P, mode);
+
+// Node i of stored level li (li < 0: leaf i).
+__device__ __forceinline__ double tval(const Model& m, const Slot& sl, int li, int i, int mode) {
+    return li < 0 ? leafv(sl, i, mode) : sl.t(m.lev_base[li] + i);
+}
+
+// Value of node i of stored level li: pairwise sum of its 2^d children.
+// ((c0+c1)+(c2+c3)) + ((c4+c5)+(c6+c7)) is exactly the binary-tree value.
+__device__ __forceinline__ double group_sum(const Model& m, const Slot& sl, int li, int i, int mode) {
+    const int d = m.lev_d[li], c0 = i << d, lc = li - 1;
+    if (d == 1) return tval(m, sl, lc, c0, mode) + tval(m, sl, lc, c0 + 1, mode);
+    if (d == 2)
+        return (tval(m, sl, lc, c0, mode) + tval(m, sl, lc, c0 + 1, mode)) +
+               (tval(m, sl, lc, c0 + 2, mode) + tval(m, sl, lc, c0 + 3, mode));
+    const double v0 = tval(m, sl, lc, c0, mode), v1 = tval(m, sl, lc, c0 + 1, mode);
+    const double v2 = tval(m, sl, lc, c0 + 2, mode), v3 = tval(m, sl, lc, c0 + 3, mode);
+    const double v4 = tval(m, sl, lc, c0 + 4, mode), v5 = tval(m, sl, lc, c0 + 5, mode);
+    const double v6 = tval(m, sl, lc, c0 + 6, mode), v7 = tval(m, sl, lc, c0 + 7, mode);
+    return ((v0 + v1) + (v2 + v3)) + ((v4 + v5) + (v6 + v7));
+}
+
+__device__ __forceinline__ double tree_root(const Model& m, const Slot& sl) {
+    return sl.t(m.lev_base[m.nlev - 1]);
 }
 
 template <int G>
-__device__ void build_tree(const Grp<G>& g, const Slot& sl, int P, int mode) {
-    for (int half = P >> 1; half >= 1; half >>= 1) {
-        for (int i = half + (int)g.lane; i < 2 * half; i += G)
-            sl.t(i) = nodev(sl, 2 * i, P, mode) + nodev(sl, 2 * i + 1, P, mode);
+__device__ void build_tree(const Grp<G>& g, const Model& m, const Slot& sl, int mode) {
+    for (int li = 0; li < m.nlev; li++) {
+        const int base = m.lev_base[li];
+        for (int i = (int)g.lane; i < m.lev_count[li]; i += G) sl.t(base + i) = group_sum(m, sl, li, i, mode);
         g.sync();
     }
 }
 
-// Leftmost leaf whose cumulative weight reaches x; never a zero leaf.
-__device__ __forceinline__ int descend(const Slot& sl, int P, double x, int mode) {
-    int node = 1;
-    while (node < P) {
-        int l = 2 * node;
-        double L = nodev(sl, l, P, mode), Rv = nodev(sl, l + 1, P, mode);
-        if ((x <= L && L > 0.0) || Rv == 0.0) {
-            node = l;
+// One binary level: left unless the target lies beyond a positive left
+// weight and the right weight is positive.
+__device__ __forceinline__ bool go_right(double& x, double L, double R) {
+    if ((x <= L && L > 0.0) || R == 0.0) return false;
+    x = x - L;
+    return true;
+}
+
+// Leftmost leaf whose cumulative weight reaches x (ties go left); never a
+// zero leaf.  Same decisions as a level-by-level descent of the binary tree.
+__device__ __forceinline__ int descend(const Model& m, const Slot& sl, double x, int mode) {
+    int i = 0;
+    for (int li = m.nlev - 1; li >= 0; li--) {
+        const int d = m.lev_d[li], c0 = i << d, lc = li - 1;
+        int j;
+        if (d == 1) {
+            j = go_right(x, tval(m, sl, lc, c0, mode), tval(m, sl, lc, c0 + 1, mode)) ? 1 : 0;
+        } else if (d == 2) {
+            const double v0 = tval(m, sl, lc, c0, mode), v1 = tval(m, sl, lc, c0 + 1, mode);
+            const double v2 = tval(m, sl, lc, c0 + 2, mode), v3 = tval(m, sl, lc, c0 + 3, mode);
+            const bool s1 = go_right(x, v0 + v1, v2 + v3);
+            const bool s2 = go_right(x, s1 ? v2 : v0, s1 ? v3 : v1);
+            j = (s1 ? 2 : 0) + (s2 ? 1 : 0);
         } else {
-            x = x - L;
-            node = l + 1;
+            const double v0 = tval(m, sl, lc, c0, mode), v1 = tval(m, sl, lc, c0 + 1, mode);
+            const double v2 = tval(m, sl, lc, c0 + 2, mode), v3 = tval(m, sl, lc, c0 + 3, mode);
+            const double v4 = tval(m, sl, lc, c0 + 4, mode), v5 = tval(m, sl, lc, c0 + 5, mode);
+            const double v6 = tval(m, sl, lc, c0 + 6, mode), v7 = tval(m, sl, lc, c0 + 7, mode);
+            const bool s1 = go_right(x, (v0 + v1) + (v2 + v3), (v4 + v5) + (v6 + v7));
+            const double a0 = s1 ? v4 : v0, a1 = s1 ? v5 : v1, a2 = s1 ? v6 : v2, a3 = s1 ? v7 : v3;
+            const bool s2 = go_right(x, a0 + a1, a2 + a3);
+            const bool s3 = go_right(x, s2 ? a2 : a0, s2 ? a3 : a1);
+            j = (s1 ? 4 : 0) + (s2 ? 2 : 0) + (s3 ? 1 : 0);
         }
+        i = c0 + j;
     }
-    return node - P;
+    return i;
 }
 
 template <int G>
 __device__ __forceinline__ void all_props(const Grp<G>& g, const Model& m, const Slot& sl) {
     for (int r = (int)g.lane; r < m.R; r += G) sl.pa(r) = prop(m, sl, r);
     g.sync();
-    build_tree<G>(g, sl, m.P, 0);
+    build_tree<G>(g, m, sl, 0);
 }
 
 // After firing r: new propensities for the reactions that depend on the
@@ -393,15 +477,18 @@ __device__ void update_after_fire(const Grp<G>& g, const Model& m, const Slot& s
         sl.pa(rr) = prop(m, sl, rr);
     }
     g.sync();
-    const int P = m.P;
-    if (nd * (uint32_t)m.logP >= (uint32_t)P) {
-        build_tree<G>(g, sl, P, 0);
+    if (nd >= (uint32_t)m.lev_count[0]) {  // touches about every bottom group: rebuild
+        build_tree<G>(g, m, sl, 0);
         return;
     }
-    for (int lev = 1; lev <= m.logP; lev++) {
+    for (int li = 0; li < m.nlev; li++) {
+        const int sh = m.lev_shift[li], base = m.lev_base[li];
+        int prev = -1;  // dependency lists are sorted: equal ancestors are adjacent
         for (uint32_t j = d0 + g.lane; j < d1; j += G) {
-            int node = (P + (int)m.dep_ent[j]) >> lev;
-            sl.t(node) = nodev(sl, 2 * node, P, 0) + nodev(sl, 2 * node + 1, P, 0);
+            const int i = (int)m.dep_ent[j] >> sh;
+            if (i == prev) continue;
+            prev = i;
+            sl.t(base + i) = group_sum(m, sl, li, i, 0);
         }
         g.sync();
     }
@@ -428,285 +515,440 @@ __device__ void finish_zero(const Grp<G>& g, const Model& m, const Run& run, con
     cursor = ns;
 }
 
-// ---------------------------------------------------------------------------
-// One simulation, start to end, by one group
-// ---------------------------------------------------------------------------
+// Scalars of one simulation while a group works on it (identical in every
+// lane of the group, except `fire`, each lane's share of the firings).
+struct Sim {
+    double T, tl, t_next;
+    unsigned long long fire;
+    uint32_t sim, cursor, n, burst, leaps, ssa, rej, status;
+    bool in_ssa;
+    uint4 wc;         // Philox block of the current SSA step pair (not persisted)
+    uint32_t wc_blk;  // its block index, or 0xffffffff
+};
+
+constexpr int CONT = 0, DONE = 1;
 
 template <int G>
-__device__ void run_sim(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl,
-                        uint32_t sim) {
-    const int S = m.S, R = m.R, P = m.P, so = m.s_out;
-    const uint32_t ns = (uint32_t)m.ns;
-    const uint32_t fl = run.flags;
-    const bool force = (fl & F_FORCE_SSA) != 0;
-    const uint32_t simg = run.sim_base + sim;
-    const uint32_t lane = g.lane;
-    uint32_t* out = run.out + (size_t)sim * ns * (size_t)so;
-
+__device__ void init_sim(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl, Sim& st,
+                         uint32_t sim) {
+    const int S = m.S, R = m.R, P = m.P;
     g.sync();
-    for (int s = (int)lane; s < S; s += G) sl.x(s) = run.X0[(size_t)sim * S + s];
-    for (int r = (int)lane; r < P; r += G) {
-        sl.cf(r) = r < R ? run.c[(size_t)sim * R + r] : 0.0f;
+    for (int s = (int)g.lane; s < S; s += G) sl.x(s) = run.X0[(size_t)sim * S + s];
+    for (int r = (int)g.lane; r < P; r += G) {
+        if (!run.uniform_c) sl.cf(r) = r < R ? run.c[(size_t)sim * R + r] : 0.0f;
         sl.pa(r) = 0.0f;
         sl.cr(r) = 0;
     }
     g.sync();
     all_props<G>(g, m, sl);
+    st.T = 0.0;
+    st.tl = 0.0;
+    st.t_next = m.tvec[0];
+    st.fire = 0ull;
+    st.sim = sim;
+    st.cursor = st.n = st.burst = st.leaps = st.ssa = st.rej = 0u;
+    st.status = CTL_SIM_OK;
+    st.in_ssa = (run.flags & F_FORCE_SSA) != 0;
+    st.wc_blk = 0xffffffffu;
+}
 
-    double T = 0.0, tl = 0.0;
-    uint32_t cursor = 0, n = 0, burst = 0, status = CTL_SIM_OK;
-    uint32_t leaps = 0, ssa = 0, rej = 0;
-    unsigned long long fire = 0;  // lane-local share of the firings
-    bool in_ssa = force;
-    double t_next = m.tvec[0];
-
-    for (;;) {
-        if (!in_ssa) {
-            // ---------------- PreCalculations: decide, then one leap ----------------
-            if (T >= m.tmax) break;
-            if (n >= run.max_steps) { status = CTL_SIM_STEP_LIMIT; break; }
-            const uint32_t step = n++;
-            const double A0 = sl.t(1);
-            if (A0 == 0.0) {
-                finish_zero<G>(g, m, run, sl, out, cursor);
-                T = m.tmax + (double)0.1f;
-                break;
-            }
-            bool lany = false;
-            for (int r = (int)lane; r < R; r += G) {
-                uint8_t cr = 0;
-                const uint32_t e1 = m.reac_off[r + 1];
-                for (uint32_t e = m.reac_off[r]; e < e1; e++) {
-                    const uint32_t ent = m.reac_ent[e];
-                    const uint32_t q = (uint32_t)sl.x((int)(ent >> 8)) / (ent & 0xffu);
-                    if ((fl & F_Q6_OFF) ? (q < run.nc) : (q > 0u && q < run.nc)) cr = 1;
-                }
-                sl.cr(r) = cr;
-                lany |= cr != 0;
-            }
-            const bool anycrit = g.any(lany);
-            g.sync();
-            float t1 = FLT_MAX;
-            for (int s = (int)lane; s < S; s += G) {
-                const uint32_t e0 = m.v_off[s], e1 = m.v_off[s + 1];
-                if (e0 == e1) continue;
-                float mu = 0.0f, sg = 0.0f;
-                for (uint32_t e = e0; e < e1; e++) {
-                    const uint32_t ent = m.v_ent[e];
-                    const int r = (int)(ent >> 8);
-                    if (sl.cr(r)) continue;
-                    const float fv = (float)(int8_t)(ent & 0xffu);
-                    mu = mu + fv * sl.pa(r);
-                    sg = sg + (fv * fv) * sl.pa(r);
-                }
-                const int32_t xs = sl.x(s);
-                const float gg = gfun(m.hor[s], m.hort[s], xs);
-                const float tmp2 = (run.eps * (float)xs) / gg;
-                const float macs = tmp2 > 1.0f ? tmp2 : 1.0f;
-                const bool use = (fl & F_Q9_OFF) ? (sg != 0.0f) : (mu != 0.0f && sg != 0.0f);
-                if (use) {
-                    const float t3 = mu != 0.0f ? macs / fabsf(mu) : __int_as_float(0x7f800000);
-                    const float t4 = (macs * macs) / sg;
-                    const float tt = t3 < t4 ? t3 : t4;
-                    if (tt < t1) t1 = tt;
-                }
-            }
-            const float tau1 = g.fmin(t1);
-            if ((double)tau1 < run.ssa_factor / A0) {
-                in_ssa = true;
-                burst = 0;
-                tl = 0.0;
-                continue;
-            }
-            double a0c = 0.0;
-            if (anycrit) {
-                build_tree<G>(g, sl, P, 1);
-                a0c = sl.t(1);
-            }
-            const uint4 wd = draw(run.seed, 0u, TAG_MISC, step, simg);
-            double tau2 = (double)FLT_MAX;
-            if (a0c > 0.0) tau2 = -dlog(u53(wd.x, wd.y)) / a0c;
-            double tau = (double)tau1 < tau2 ? (double)tau1 : tau2;
-            int pick = -1;
-            if ((double)tau1 > tau2) {
-                int mode = 1;
-                if (!(fl & F_Q2_OFF) && !sl.cr(0)) {
-                    mode = 2;
-                    if (lane == 0)
-                        for (int i = P >> 1; i >= 1; i >>= 1) sl.t(i) = nodev(sl, 2 * i, P, 2) + nodev(sl, 2 * i + 1, P, 2);
-                    g.sync();
-                }
-                pick = descend(sl, P, u53(wd.z, wd.w) * a0c, mode);
-            }
-            uint32_t attempt = 0;
-            bool ovf = false;
-            for (;;) {
-                const bool keep = attempt == 0 || (fl & F_Q3_OFF);
-                for (uint32_t pb = lane; 2u * pb < (uint32_t)R; pb += G) {
-                    const int r0 = (int)(2u * pb), r1 = r0 + 1;
-                    const bool c0 = sl.cr(r0) != 0;
-                    const bool c1 = r1 < R ? sl.cr(r1) != 0 : true;
-                    const double l0 = c0 ? 0.0 : tau * (double)sl.pa(r0);
-                    const double l1 = (c1 || r1 >= R) ? 0.0 : tau * (double)sl.pa(r1);
-                    const uint32_t tg = tag_pois(attempt, pb);
-                    uint4 w = make_uint4(0u, 0u, 0u, 0u);
-                    if (l0 > 0.0 || l1 > 0.0) w = draw(run.seed, 0u, tg, step, simg);
-                    sl.k(r0) = c0 ? ((r0 == pick && keep) ? 1u : 0u)
-                                  : poisson(l0, w.x, w.y, run.seed, tg, step, simg, 0u);
-                    if (r1 < R)
-                        sl.k(r1) = c1 ? ((r1 == pick && keep) ? 1u : 0u)
-                                      : poisson(l1, w.z, w.w, run.seed, tg, step, simg, 1u);
-                }
-                g.sync();
-                bool lfail = false, lovf = false;
-                for (int s = (int)lane; s < S; s += G) {
-                    int64_t x1 = sl.x(s);
-                    const uint32_t e1 = m.fs_off[s + 1];
-                    for (uint32_t e = m.fs_off[s]; e < e1; e++) {
-                        const uint32_t ent = m.fs_ent[e];
-                        x1 += (int64_t)(int8_t)(ent & 0xffu) * (int64_t)sl.k((int)(ent >> 8));
-                        if (!(fl & F_Q4_OFF) && x1 < 0) { lfail = true; break; }
-                    }
-                    if (x1 < 0) lfail = true;
-                    if (x1 > 2147483647LL) lovf = true;
-                    sl.x1(s) = (int32_t)x1;
-                }
-                const bool fail = g.any(lfail);
-                g.sync();
-                if (!fail) {
-                    ovf = g.any(lovf);
-                    break;
-                }
-                tau = tau * 0.5;
-                attempt++;
-                rej++;
-                if (attempt >= MAX_ATTEMPTS) { status = CTL_SIM_ATTEMPT_LIMIT; break; }
-            }
-            if (status != CTL_SIM_OK) break;
-            if (ovf) { status = CTL_SIM_OVERFLOW; break; }
-            // check_time_instant (tau.cu:1507-1562)
-            while (cursor < ns && T + tau >= t_next) {
-                for (int k = (int)lane; k < so; k += G) {
-                    const int s = (int)m.cs[k];
-                    const int32_t xs = sl.x(s);
-                    const double d = (double)((int64_t)sl.x1(s) - (int64_t)xs);
-                    const double delta = (d * (t_next - T)) / tau;
-                    const double ri = rint(delta);
-                    uint32_t v;
-                    if (!(fl & F_Q1_OFF))
-                        v = (uint32_t)xs + (ri > 0.0 ? (uint32_t)ri : 0u);
-                    else
-                        v = (uint32_t)((int64_t)xs + (int64_t)ri);
-                    out[(size_t)cursor * so + k] = v;
-                }
-                cursor++;
-                t_next = cursor < ns ? m.tvec[cursor] : 0.0;
-            }
-            unsigned long long fs = 0;
-            for (int r = (int)lane; r < R; r += G) fs += sl.k(r);
-            fire += fs;
-            leaps++;
-            g.sync();
-            for (int s = (int)lane; s < S; s += G) sl.x(s) = sl.x1(s);
-            g.sync();
-            T = T + tau;
-            all_props<G>(g, m, sl);
-            if (cursor == ns) break;
-        } else {
-            // ---------------- EventualSSASteps / LightweightSSA: one step ----------------
-            if (n >= run.max_steps) { status = CTL_SIM_STEP_LIMIT; break; }
-            const double A0 = sl.t(1);
-            if (A0 == 0.0) {
-                finish_zero<G>(g, m, run, sl, out, cursor);
-                T = m.tmax + (double)0.1f;
-                break;
-            }
-            const uint32_t step = n++;
-            const uint4 wd = draw(run.seed, 0u, TAG_SSA, step, simg);
-            const int r = descend(sl, P, u53(wd.x, wd.y) * A0, 0);
-            const double dt = -dlog(u53(wd.z, wd.w)) / A0;
-            tl = tl + dt;
-            while (cursor < ns && T + tl > t_next) {
-                for (int k = (int)lane; k < so; k += G) out[(size_t)cursor * so + k] = (uint32_t)sl.x((int)m.cs[k]);
-                cursor++;
-                t_next = cursor < ns ? m.tvec[cursor] : 0.0;
-            }
-            g.sync();
-            bool lovf = false;
-            const uint32_t e1 = m.fr_off[r + 1];
-            for (uint32_t e = m.fr_off[r] + lane; e < e1; e += G) {
-                const uint32_t ent = m.fr_ent[e];
-                const int s = (int)(ent >> 8);
-                const int64_t nx = (int64_t)sl.x(s) + (int64_t)(int8_t)(ent & 0xffu);
-                if (nx > 2147483647LL || nx < 0) lovf = true;
-                sl.x(s) = (int32_t)nx;
-            }
-            const bool ovf = g.any(lovf);
-            ssa++;
-            if (lane == 0) fire += 1ull;
-            if (ovf) { status = CTL_SIM_OVERFLOW; break; }
-            g.sync();
-            update_after_fire<G>(g, m, sl, r);
-            burst++;
-            if (cursor == ns) break;
-            if (burst == run.ssa_steps) {
-                T = T + tl;
-                tl = 0.0;
-                burst = 0;
-                if (!force) in_ssa = false;
-                else if (T >= m.tmax) break;
-            }
+// PreCalculations (tau.cu:1568-2093): the SSA hand-off decision and, unless
+// it hands off, one Cao tau-leap with critical reactions and rejection.
+template <int G>
+__device__ int decide_step(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl, Sim& st,
+                           uint32_t* out) {
+    const int S = m.S, R = m.R, so = m.s_out;
+    const uint32_t ns = (uint32_t)m.ns;
+    const uint32_t fl = run.flags;
+    const uint32_t lane = g.lane;
+    const uint32_t simg = run.sim_base + st.sim;
+    if (st.T >= m.tmax) return DONE;
+    if (st.n >= run.max_steps) { st.status = CTL_SIM_STEP_LIMIT; return DONE; }
+    const uint32_t step = st.n++;
+    const double A0 = tree_root(m, sl);
+    if (A0 == 0.0) {
+        finish_zero<G>(g, m, run, sl, out, st.cursor);
+        st.T = m.tmax + (double)0.1f;
+        return DONE;
+    }
+    bool lany = false;
+    for (int r = (int)lane; r < R; r += G) {
+        uint8_t cr = 0;
+        const uint32_t e1 = m.reac_off[r + 1];
+        for (uint32_t e = m.reac_off[r]; e < e1; e++) {
+            const uint32_t ent = m.reac_ent[e];
+            const uint32_t q = (uint32_t)sl.x((int)(ent >> 8)) / (ent & 0xffu);
+            if ((fl & F_Q6_OFF) ? (q < run.nc) : (q > 0u && q < run.nc)) cr = 1;
+        }
+        sl.cr(r) = cr;
+        lany |= cr != 0;
+    }
+    const bool anycrit = g.any(lany);
+    g.sync();
+    float t1 = FLT_MAX;
+    for (int s = (int)lane; s < S; s += G) {
+        const uint32_t e0 = m.v_off[s], e1 = m.v_off[s + 1];
+        if (e0 == e1) continue;
+        float mu = 0.0f, sg = 0.0f;
+        for (uint32_t e = e0; e < e1; e++) {
+            const uint32_t ent = m.v_ent[e];
+            const int r = (int)(ent >> 8);
+            if (sl.cr(r)) continue;
+            const float fv = (float)(int8_t)(ent & 0xffu);
+            mu = mu + fv * sl.pa(r);
+            sg = sg + (fv * fv) * sl.pa(r);
+        }
+        const int32_t xs = sl.x(s);
+        const float gg = gfun(m.hor[s], m.hort[s], xs);
+        const float tmp2 = (run.eps * (float)xs) / gg;
+        const float macs = tmp2 > 1.0f ? tmp2 : 1.0f;
+        const bool use = (fl & F_Q9_OFF) ? (sg != 0.0f) : (mu != 0.0f && sg != 0.0f);
+        if (use) {
+            const float t3 = mu != 0.0f ? macs / fabsf(mu) : __int_as_float(0x7f800000);
+            const float t4 = (macs * macs) / sg;
+            const float tt = t3 < t4 ? t3 : t4;
+            if (tt < t1) t1 = tt;
         }
     }
-    for (uint32_t i = cursor; i < ns; i++)
-        for (int k = (int)lane; k < so; k += G) out[(size_t)i * so + k] = 0u;
-    const unsigned long long ftot = g.sum(fire);
-    if (lane == 0) {
+    const float tau1 = g.fmin(t1);
+    if ((double)tau1 < run.ssa_factor / A0) {
+        st.in_ssa = true;
+        st.burst = 0;
+        st.tl = 0.0;
+        return CONT;
+    }
+    double a0c = 0.0;
+    if (anycrit) {
+        build_tree<G>(g, m, sl, 1);
+        a0c = tree_root(m, sl);
+    }
+    const uint4 wd = draw(run.seed, 0u, TAG_MISC, step, simg);
+    double tau2 = (double)FLT_MAX;
+    if (a0c > 0.0) tau2 = -dlog(u53(wd.x, wd.y)) / a0c;
+    double tau = (double)tau1 < tau2 ? (double)tau1 : tau2;
+    int pick = -1;
+    if ((double)tau1 > tau2) {
+        int mode = 1;
+        if (!(fl & F_Q2_OFF) && !sl.cr(0)) {
+            mode = 2;
+            if (lane == 0)  // the ancestors of leaf 0 are node 0 of every stored level
+                for (int li = 0; li < m.nlev; li++) sl.t(m.lev_base[li]) = group_sum(m, sl, li, 0, 2);
+            g.sync();
+        }
+        pick = descend(m, sl, u53(wd.z, wd.w) * a0c, mode);
+    }
+    uint32_t attempt = 0;
+    bool ovf = false;
+    for (;;) {
+        const bool keep = attempt == 0 || (fl & F_Q3_OFF);
+        for (uint32_t pb = lane; 2u * pb < (uint32_t)R; pb += G) {
+            const int r0 = (int)(2u * pb), r1 = r0 + 1;
+            const bool c0 = sl.cr(r0) != 0;
+            const bool c1 = r1 < R ? sl.cr(r1) != 0 : true;
+            const double l0 = c0 ? 0.0 : tau * (double)sl.pa(r0);
+            const double l1 = (c1 || r1 >= R) ? 0.0 : tau * (double)sl.pa(r1);
+            const uint32_t tg = tag_pois(attempt, pb);
+            uint4 w = make_uint4(0u, 0u, 0u, 0u);
+            if (l0 > 0.0 || l1 > 0.0) w = draw(run.seed, 0u, tg, step, simg);
+            sl.k(r0) = c0 ? ((r0 == pick && keep) ? 1u : 0u)
+                          : poisson(l0, w.x, w.y, run.seed, tg, step, simg, 0u);
+            if (r1 < R)
+                sl.k(r1) = c1 ? ((r1 == pick && keep) ? 1u : 0u)
+                              : poisson(l1, w.z, w.w, run.seed, tg, step, simg, 1u);
+        }
+        g.sync();
+        bool lfail = false, lovf = false;
+        for (int s = (int)lane; s < S; s += G) {
+            int64_t x1 = sl.x(s);
+            const uint32_t e1 = m.fs_off[s + 1];
+            for (uint32_t e = m.fs_off[s]; e < e1; e++) {
+                const uint32_t ent = m.fs_ent[e];
+                x1 += (int64_t)(int8_t)(ent & 0xffu) * (int64_t)sl.k((int)(ent >> 8));
+                if (!(fl & F_Q4_OFF) && x1 < 0) { lfail = true; break; }
+            }
+            if (x1 < 0) lfail = true;
+            if (x1 > 2147483647LL) lovf = true;
+            sl.x1(s) = (int32_t)x1;
+        }
+        const bool fail = g.any(lfail);
+        g.sync();
+        if (!fail) {
+            ovf = g.any(lovf);
+            break;
+        }
+        tau = tau * 0.5;
+        attempt++;
+        st.rej++;
+        if (attempt >= MAX_ATTEMPTS) { st.status = CTL_SIM_ATTEMPT_LIMIT; return DONE; }
+    }
+    if (ovf) { st.status = CTL_SIM_OVERFLOW; return DONE; }
+    // check_time_instant (tau.cu:1507-1562)
+    const double T = st.T;
+    while (st.cursor < ns && T + tau >= st.t_next) {
+        for (int k = (int)lane; k < so; k += G) {
+            const int s = (int)m.cs[k];
+            const int32_t xs = sl.x(s);
+            const double d = (double)((int64_t)sl.x1(s) - (int64_t)xs);
+            const double delta = (d * (st.t_next - T)) / tau;
+            const double ri = rint(delta);
+            uint32_t v;
+            if (!(fl & F_Q1_OFF))
+                v = (uint32_t)xs + (ri > 0.0 ? (uint32_t)ri : 0u);
+            else
+                v = (uint32_t)((int64_t)xs + (int64_t)ri);
+            out[(size_t)st.cursor * so + k] = v;
+        }
+        st.cursor++;
+        st.t_next = st.cursor < ns ? m.tvec[st.cursor] : 0.0;
+    }
+    unsigned long long fs = 0;
+    for (int r = (int)lane; r < R; r += G) fs += sl.k(r);
+    st.fire += fs;
+    st.leaps++;
+    g.sync();
+    for (int s = (int)lane; s < S; s += G) sl.x(s) = sl.x1(s);
+    g.sync();
+    st.T = T + tau;
+    all_props<G>(g, m, sl);
+    return st.cursor == ns ? DONE : CONT;
+}
+
+// EventualSSASteps / LightweightSSA (tau.cu:2099-2454): one direct-method step.
+template <int G>
+__device__ int ssa_step(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl, Sim& st,
+                        uint32_t* out) {
+    const int so = m.s_out;
+    const uint32_t ns = (uint32_t)m.ns;
+    const uint32_t lane = g.lane;
+    if (st.n >= run.max_steps) { st.status = CTL_SIM_STEP_LIMIT; return DONE; }
+    const double A0 = tree_root(m, sl);
+    if (A0 == 0.0) {
+        finish_zero<G>(g, m, run, sl, out, st.cursor);
+        st.T = m.tmax + (double)0.1f;
+        return DONE;
+    }
+    const uint32_t step = st.n++;
+    // one Philox block per two SSA steps: (w0,w1) for even steps, (w2,w3)
+    // for odd ones; 32-bit pick uniform, FP32 waiting time
+    if (st.wc_blk != (step >> 1)) {
+        st.wc = draw(run.seed, 0u, TAG_SSA, step >> 1, run.sim_base + st.sim);
+        st.wc_blk = step >> 1;
+    }
+    const uint32_t wa = (step & 1u) ? st.wc.z : st.wc.x, wb = (step & 1u) ? st.wc.w : st.wc.y;
+    const int r = descend(m, sl, u32d(wa) * A0, 0);
+    const float dtf = -flog(u24f(wb)) / (float)A0;
+    st.tl = st.tl + (double)dtf;
+    while (st.cursor < ns && st.T + st.tl > st.t_next) {
+        for (int k = (int)lane; k < so; k += G) out[(size_t)st.cursor * so + k] = (uint32_t)sl.x((int)m.cs[k]);
+        st.cursor++;
+        st.t_next = st.cursor < ns ? m.tvec[st.cursor] : 0.0;
+    }
+    g.sync();
+    bool lovf = false;
+    const uint32_t e1 = m.fr_off[r + 1];
+    for (uint32_t e = m.fr_off[r] + lane; e < e1; e += G) {
+        const uint32_t ent = m.fr_ent[e];
+        const int s = (int)(ent >> 8);
+        const int64_t nx = (int64_t)sl.x(s) + (int64_t)(int8_t)(ent & 0xffu);
+        if (nx > 2147483647LL || nx < 0) lovf = true;
+        sl.x(s) = (int32_t)nx;
+    }
+    const bool ovf = g.any(lovf);
+    st.ssa++;
+    if (lane == 0) st.fire += 1ull;
+    if (ovf) { st.status = CTL_SIM_OVERFLOW; return DONE; }
+    g.sync();
+    update_after_fire<G>(g, m, sl, r);
+    st.burst++;
+    if (st.cursor == ns) return DONE;
+    if (st.burst == run.ssa_steps) {
+        st.T = st.T + st.tl;
+        st.tl = 0.0;
+        st.burst = 0;
+        if (!(run.flags & F_FORCE_SSA)) st.in_ssa = false;
+        else if (st.T >= m.tmax) return DONE;
+    }
+    return CONT;
+}
+
+template <int G>
+__device__ void finish_sim(const Grp<G>& g, const Model& m, const Run& run, const Sim& st, uint32_t* out) {
+    const int so = m.s_out;
+    for (uint32_t i = st.cursor; i < (uint32_t)m.ns; i++)
+        for (int k = (int)g.lane; k < so; k += G) out[(size_t)i * so + k] = 0u;
+    const unsigned long long ftot = g.sum(st.fire);
+    if (g.lane == 0) {
         ctl_sim_info inf;
-        inf.t_final = T + tl;
+        inf.t_final = st.T + st.tl;
         inf.firings = ftot;
-        inf.status = status;
-        inf.steps = n;
-        inf.leaps = leaps;
-        inf.ssa_steps = ssa;
-        inf.rejections = rej;
+        inf.status = st.status;
+        inf.steps = st.n;
+        inf.leaps = st.leaps;
+        inf.ssa_steps = st.ssa;
+        inf.rejections = st.rej;
         inf.pad = 0;
-        run.info[sim] = inf;
+        run.info[st.sim] = inf;
     }
 }
 
 template <int G>
-__global__ void __launch_bounds__(256) sweep_kernel(Model m, Run run, Layout lay) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int NS = (int)(blockDim.x / G);
-    const int j = (int)(threadIdx.x / G);
-    Grp<G> g;
+__device__ __forceinline__ void load_sim(const Grp<G>& g, const StateArrays& sa, int j, Sim& st) {
+    st.T = sa.T[j];
+    st.tl = sa.tl[j];
+    st.t_next = sa.tnext[j];
+    st.fire = g.lane == 0 ? sa.fire[j] : 0ull;
+    st.sim = sa.sim[j];
+    st.cursor = sa.cursor[j];
+    st.n = sa.n[j];
+    st.burst = sa.burst[j];
+    st.leaps = sa.leaps[j];
+    st.ssa = sa.ssa[j];
+    st.rej = sa.rej[j];
+    const uint32_t f = sa.flags[j];
+    st.in_ssa = (f & ST_IN_SSA) != 0;
+    st.status = f >> ST_STATUS_SHIFT;
+    st.wc_blk = 0xffffffffu;
+}
+
+template <int G>
+__device__ __forceinline__ void store_sim(const Grp<G>& g, const StateArrays& sa, int j, const Sim& st) {
+    const unsigned long long f = g.sum(st.fire);
+    if (g.lane == 0) {
+        sa.T[j] = st.T;
+        sa.tl[j] = st.tl;
+        sa.tnext[j] = st.t_next;
+        sa.fire[j] = f;
+        sa.sim[j] = st.sim;
+        sa.cursor[j] = st.cursor;
+        sa.n[j] = st.n;
+        sa.burst[j] = st.burst;
+        sa.leaps[j] = st.leaps;
+        sa.ssa[j] = st.ssa;
+        sa.rej[j] = st.rej;
+        sa.flags[j] = (st.in_ssa ? ST_IN_SSA : 0u) | (st.status << ST_STATUS_SHIFT);
+    }
+}
+
+template <int G>
+__device__ __forceinline__ Slot slot_of(unsigned char* smem, const Layout& lay, int j, int NS, bool uniform_c) {
     Slot sl;
     if (G == 1) {
         sl.st = NS;
         sl.X = reinterpret_cast<int32_t*>(smem + lay.off_X) + j;
         sl.X1 = reinterpret_cast<int32_t*>(smem + lay.off_X1) + j;
         sl.a = reinterpret_cast<float*>(smem + lay.off_a) + j;
-        sl.tree = reinterpret_cast<double*>(smem + lay.off_tree) + j;
         sl.K = reinterpret_cast<uint32_t*>(smem + lay.off_K) + j;
+        sl.tree = reinterpret_cast<double*>(smem + lay.off_tree) + j;
         sl.crit = reinterpret_cast<uint8_t*>(smem + lay.off_crit) + j;
-        sl.c = reinterpret_cast<float*>(smem + lay.off_c) + j;
+        sl.c = reinterpret_cast<float*>(smem + lay.off_c) + (uniform_c ? 0 : j);
+        sl.cst = uniform_c ? 1 : NS;
     } else {
         sl.st = 1;
         sl.X = reinterpret_cast<int32_t*>(smem + lay.off_X) + (size_t)j * lay.len_S;
         sl.X1 = reinterpret_cast<int32_t*>(smem + lay.off_X1) + (size_t)j * lay.len_S;
         sl.a = reinterpret_cast<float*>(smem + lay.off_a) + (size_t)j * lay.len_P;
-        sl.tree = reinterpret_cast<double*>(smem + lay.off_tree) + (size_t)j * lay.len_P;
         sl.K = reinterpret_cast<uint32_t*>(smem + lay.off_K) + (size_t)j * lay.len_P;
+        sl.tree = reinterpret_cast<double*>(smem + lay.off_tree) + (size_t)j * lay.len_T;
         sl.crit = reinterpret_cast<uint8_t*>(smem + lay.off_crit) + (size_t)j * lay.len_C;
-        sl.c = reinterpret_cast<float*>(smem + lay.off_c) + (size_t)j * lay.len_P;
+        sl.c = reinterpret_cast<float*>(smem + lay.off_c) + (uniform_c ? 0 : (size_t)j * lay.len_P);
+        sl.cst = 1;
     }
+    return sl;
+}
+
+// Persistent sweep.  Every round: (1) each group refills its own slot from
+// the device work queue when it is empty; (2) the block sorts the occupied
+// slots into an SSA list and a decision/leap list (shared-memory atomics);
+// (3) groups take list entries, so every warp executes one phase only
+// (regrouping), and advance each taken simulation by a bounded amount of
+// work.  The loop ends when the queue is drained and every slot is closed.
+template <int G>
+__global__ void __launch_bounds__(256) sweep_kernel(Model m, Run run, Layout lay) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t s_cnt[2];
+    const int NS = (int)(blockDim.x / G);
+    const int gi = (int)(threadIdx.x / G);
+    Grp<G> g;
+    StateArrays sa;
+    {
+        unsigned char* b = smem + lay.off_state;
+        sa.T = reinterpret_cast<double*>(b);
+        sa.tl = sa.T + NS;
+        sa.tnext = sa.tl + NS;
+        sa.fire = reinterpret_cast<unsigned long long*>(sa.tnext + NS);
+        uint32_t* u = reinterpret_cast<uint32_t*>(sa.fire + NS);
+        sa.sim = u;
+        sa.cursor = u + NS;
+        sa.n = u + 2 * NS;
+        sa.burst = u + 3 * NS;
+        sa.leaps = u + 4 * NS;
+        sa.ssa = u + 5 * NS;
+        sa.rej = u + 6 * NS;
+        sa.flags = u + 7 * NS;
+    }
+    uint32_t* phase = sa.flags + NS;
+    uint32_t* list = reinterpret_cast<uint32_t*>(smem + lay.off_list);
+    const bool uni = run.uniform_c != 0;
+    if (uni) {
+        float* cs = reinterpret_cast<float*>(smem + lay.off_c);
+        for (int r = (int)threadIdx.x; r < m.P; r += (int)blockDim.x) cs[r] = r < m.R ? run.c[r] : 0.0f;
+    }
+    for (int j = (int)threadIdx.x; j < NS; j += (int)blockDim.x) phase[j] = PH_EMPTY;
+    __syncthreads();
+    const uint32_t ns = (uint32_t)m.ns;
+    const size_t sim_stride = (size_t)ns * (size_t)m.s_out;
     for (;;) {
-        uint32_t sim = 0;
-        if (g.lane == 0) sim = atomicAdd(run.queue, 1u);
-        sim = g.bcast(sim);
-        if (sim >= run.n) break;
-        run_sim<G>(g, m, run, sl, sim);
+        if (phase[gi] == PH_EMPTY) {
+            uint32_t sim = 0;
+            if (g.lane == 0) sim = atomicAdd(run.queue, 1u);
+            sim = g.bcast(sim);
+            if (sim >= run.n) {
+                if (g.lane == 0) phase[gi] = PH_CLOSED;
+            } else {
+                const Slot sl = slot_of<G>(smem, lay, gi, NS, uni);
+                Sim st;
+                init_sim<G>(g, m, run, sl, st, sim);
+                store_sim<G>(g, sa, gi, st);
+                if (g.lane == 0) phase[gi] = st.in_ssa ? PH_SSA : PH_DECIDE;
+            }
+        }
+        if (threadIdx.x == 0) {
+            s_cnt[0] = 0u;
+            s_cnt[1] = 0u;
+        }
+        __syncthreads();
+        for (int j = (int)threadIdx.x; j < NS; j += (int)blockDim.x) {
+            const uint32_t ph = phase[j];
+            if (ph == PH_SSA) list[atomicAdd(&s_cnt[0], 1u)] = (uint32_t)j;
+            else if (ph == PH_DECIDE) list[NS - 1 - (int)atomicAdd(&s_cnt[1], 1u)] = (uint32_t)j;
+        }
+        __syncthreads();
+        const uint32_t nssa = s_cnt[0], ndec = s_cnt[1];
+        if (nssa + ndec == 0u) break;
+        for (uint32_t k = (uint32_t)gi; k < nssa + ndec; k += (uint32_t)NS) {
+            const bool is_ssa = k < nssa;
+            const int j = (int)(is_ssa ? list[k] : list[NS - 1 - (int)(k - nssa)]);
+            const Slot sl = slot_of<G>(smem, lay, j, NS, uni);
+            Sim st;
+            load_sim<G>(g, sa, j, st);
+            uint32_t* out = run.out + (size_t)st.sim * sim_stride;
+            int res = CONT;
+            if (is_ssa) {
+                for (uint32_t b = 0; b < run.ssa_budget && res == CONT && st.in_ssa; b++)
+                    res = ssa_step<G>(g, m, run, sl, st, out);
+            } else {
+                for (uint32_t b = 0; b < run.dec_budget && res == CONT && !st.in_ssa; b++)
+                    res = decide_step<G>(g, m, run, sl, st, out);
+            }
+            if (res == DONE) {
+                finish_sim<G>(g, m, run, st, out);
+                if (g.lane == 0) phase[j] = PH_EMPTY;
+            } else {
+                store_sim<G>(g, sa, j, st);
+                if (g.lane == 0) phase[j] = st.in_ssa ? PH_SSA : PH_DECIDE;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -833,6 +1075,8 @@ static ctl_status ensure_device(ctl_model* m, int device, DeviceCopy*& out) {
     return CTL_OK;
 }
 
+static void tree_levels(const HostTables& t, dev::Model& dm);
+
 static dev::Model make_dev_model(const ctl_model* m, const DeviceCopy& d, uint32_t flags) {
     const HostTables& t = m->t;
     auto P = [&](size_t o) { return static_cast<const unsigned char*>(d.buf) + o; };
@@ -854,6 +1098,7 @@ static dev::Model make_dev_model(const ctl_model* m, const DeviceCopy& d, uint32
     dm.tvec = reinterpret_cast<const double*>(P(d.off_tvec));
     dm.cs = reinterpret_cast<const uint32_t*>(P(d.off_cs));
     dm.tmax = t.tmax;
+    tree_levels(t, dm);
     return dm;
 }
 
@@ -863,28 +1108,61 @@ struct LaunchPlan {
     dev::Layout lay{};
 };
 
-static size_t slot_layout(const HostTables& t, int G, int NS, dev::Layout& lay) {
+// Stored levels of the sum tree for P = 2^k leaves: 3, 6, ... below k, then
+// k (the root).  Level li is the pairwise sum of 2^d nodes of level li-1.
+static void tree_levels(const HostTables& t, dev::Model& dm) {
+    const int k = t.logP;
+    int prev = 0, base = 0, n = 0;
+    for (int l = 3; l < k; l += 3) {
+        dm.lev_shift[n] = l;
+        dm.lev_d[n] = l - prev;
+        dm.lev_base[n] = base;
+        dm.lev_count[n] = t.P >> l;
+        base += t.P >> l;
+        prev = l;
+        n++;
+    }
+    dm.lev_shift[n] = k;
+    dm.lev_d[n] = k - prev;
+    dm.lev_base[n] = base;
+    dm.lev_count[n] = 1;
+    dm.nlev = n + 1;
+}
+
+static int tree_words(const HostTables& t) {
+    dev::Model dm;
+    tree_levels(t, dm);
+    return dm.lev_base[dm.nlev - 1] + 1;
+}
+
+// Shared-memory bytes of a block with NS slots of group size G.
+static size_t slot_layout(const HostTables& t, int G, int NS, bool uniform_c, dev::Layout& lay) {
     size_t off = 0;
     auto region = [&](size_t bytes) {
         size_t o = off;
         off = align16(off + bytes);
         return (uint32_t)o;
     };
+    const int tw = tree_words(t);
     if (G == 1) {
         lay.len_S = (uint32_t)t.S;
         lay.len_P = (uint32_t)t.P;
         lay.len_C = (uint32_t)t.P;
+        lay.len_T = (uint32_t)tw;
     } else {
         lay.len_S = (uint32_t)(t.S | 1);
         lay.len_P = (uint32_t)(t.P + 1);
         lay.len_C = (uint32_t)(((t.P + 3) & ~3) + 4);
+        lay.len_T = (uint32_t)(tw | 1);
     }
-    lay.off_tree = region((size_t)NS * lay.len_P * 8);
+    lay.off_tree = region((size_t)NS * lay.len_T * 8);
+    lay.off_state = region((size_t)NS * (4 * 8 + 9 * 4));
     lay.off_X = region((size_t)NS * lay.len_S * 4);
     lay.off_X1 = region((size_t)NS * lay.len_S * 4);
     lay.off_a = region((size_t)NS * lay.len_P * 4);
     lay.off_K = region((size_t)NS * lay.len_P * 4);
-    lay.off_c = region((size_t)NS * lay.len_P * 4);
+    lay.off_c = region(uniform_c ? (size_t)t.P * 4 : (size_t)NS * lay.len_P * 4);
+    lay.off_list = region((size_t)NS * 4);
     lay.off_crit = region((size_t)NS * lay.len_C);
     return off;
 }
@@ -905,14 +1183,17 @@ static const void* kernel_for(int G) {
     return nullptr;
 }
 
+// Lanes per simulation when the caller does not choose: about 16
+// reactions per lane (measured best for 64x128: G = 8; tiny networks: 1).
 static int heuristic_group(const HostTables& t) {
-    int g = t.P / 8;
+    int g = t.P / 16;
     int G = 1;
     while (G < g && G < 32) G <<= 1;
     return G;
 }
 
 // Launch shape for (model, cfg, n): group size, threads, slots and grid.
+// Small batches use smaller blocks so that every SM gets work.
 static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, LaunchPlan& pl) {
     const HostTables& t = m->t;
     int G = cfg->group > 0 ? cfg->group : heuristic_group(t);
@@ -930,9 +1211,13 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
     cudaDeviceProp prop;
     CTL_CUDA(cudaGetDeviceProperties(&prop, dev_id));
     const size_t smem_max = prop.sharedMemPerBlockOptin;
+    const bool uni = cfg->uniform_rates != 0;
+    if (cfg->threads <= 0) {
+        while (threads > 32 && (uint64_t)n * G < (uint64_t)threads * prop.multiProcessorCount) threads -= 32;
+    }
     for (;;) {
         int NS = threads / G;
-        size_t bytes = slot_layout(t, G, NS, pl.lay);
+        size_t bytes = slot_layout(t, G, NS, uni, pl.lay);
         if (bytes <= smem_max) {
             pl.smem = bytes;
             pl.NS = NS;
@@ -979,6 +1264,9 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.max_steps = cfg->max_steps;
     run.sim_base = cfg->sim_base;
     run.n = n;
+    run.uniform_c = cfg->uniform_rates != 0;
+    run.ssa_budget = cfg->ssa_budget > 0 ? (uint32_t)cfg->ssa_budget : 8u;
+    run.dec_budget = cfg->dec_budget > 0 ? (uint32_t)cfg->dec_budget : 2u;
     run.X0 = dX0;
     run.c = dc;
     run.out = dout;
@@ -1093,6 +1381,14 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
     DeviceGuard dg(cfg->device);
     DeviceCopy* d = nullptr;
     if ((st = ensure_device(m, cfg->device, d)) != CTL_OK) return st;
+    ctl_run_cfg rc = *cfg;
+    if (!rc.uniform_rates) {  // one shared copy of c when every row equals row 0
+        bool same = true;
+        for (uint32_t i = 1; i < n && same; i++)
+            same = std::memcmp(c + (size_t)i * t.R, c, (size_t)t.R * sizeof(float)) == 0;
+        rc.uniform_rates = same ? 1 : 0;
+    }
+    cfg = &rc;
     LaunchPlan pl;
     if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;
     const size_t bx = (size_t)n * t.S * 4, bc = (size_t)n * t.R * 4;

@@ -87,6 +87,10 @@ typedef struct {
     int32_t device;       /* CUDA device ordinal                                       */
     int32_t group;        /* lanes per simulation: 1,2,4,8,16,32; 0 = autotune         */
     int32_t threads;      /* threads per block; 0 = autotune                           */
+    int32_t uniform_rates;/* 1: every row of c equals row 0 (one shared copy per block);
+                             ctl_run detects this itself, device calls take it as given */
+    int32_t ssa_budget;   /* SSA steps per simulation and scheduling round (0 = 8)     */
+    int32_t dec_budget;   /* leap decisions per simulation and round (0 = 2)           */
     int32_t reserved;
 } ctl_run_cfg;
 

@@ -66,6 +66,8 @@ def lib():
         L.ctlo_philox.argtypes = [P, P, P]
         L.ctlo_log.restype = C.c_double
         L.ctlo_log.argtypes = [C.c_double]
+        L.ctlo_logf.restype = C.c_float
+        L.ctlo_logf.argtypes = [C.c_float]
         L.ctlo_exp.restype = C.c_double
         L.ctlo_exp.argtypes = [C.c_double]
         L.ctlo_logfact.restype = C.c_double
@@ -91,6 +93,10 @@ def philox(ctr, key) -> np.ndarray:
 
 def log(x: float) -> float:
     return lib().ctlo_log(float(x))
+
+
+def logf(x: float) -> float:
+    return lib().ctlo_logf(float(x))
 
 
 def exp(x: float) -> float:

@@ -19,7 +19,7 @@
 /* ------------------------------------------------------------------------ */
 
 /* Counter word 1 ("tag") of the Philox counter (block, tag, step, sim). */
-#define TAG_SSA   0x40000000u /* SSA step: (w0,w1) pick, (w2,w3) waiting time   */
+#define TAG_SSA   0x40000000u /* SSA steps 2b, 2b+1: block b, (w0,w1) / (w2,w3)   */
 #define TAG_MISC  0x40000001u /* leap: (w0,w1) tau2, (w2,w3) critical pick      */
 #define TAG_GILL  0x20000000u /* exact Gillespie oracle                        */
 #define TAG_POIS(attempt, pair) (0x80000000u | ((uint32_t)(attempt) << 20) | (uint32_t)(pair))
@@ -132,6 +132,34 @@ double ctlo_exp(double x) {
     if (ki < -1000) { p = p * 0x1p-200; ki = ki + 200; }
     return p * u2d((uint64_t)(ki + 1023) << 52);
 }
+
+/* FP32 log(x) for normal x > 0: the same reduction as ctlo_log in single
+ * precision, series 2s(1 + s^2/3 + s^4/5 + s^6/7 + s^8/9). */
+#define LN2_HI_F 0x1.62e4p-1f       /* ln 2 rounded to 16 significant bits */
+#define LN2_LO_F 0x1.7f7d1cp-20f   /* ln 2 - LN2_HI_F, rounded */
+float ctlo_logf(float x) {
+    uint32_t b;
+    memcpy(&b, &x, 4);
+    int e = (int)((b >> 23) & 0xff) - 127;
+    uint32_t mb = (b & 0x007fffffu) | 0x3f800000u;
+    float m;
+    memcpy(&m, &mb, 4);
+    if (m > 0x1.6a09e6p+0f) { m = m * 0.5f; e = e + 1; }
+    float f = m - 1.0f;
+    float sv = f / (2.0f + f);
+    float z = sv * sv;
+    float p = 0x1.c71c72p-4f;             /* 1/9 */
+    p = fmaf(p, z, 0x1.24924ap-3f);       /* 1/7 */
+    p = fmaf(p, z, 0x1.99999ap-3f);       /* 1/5 */
+    p = fmaf(p, z, 0x1.555556p-2f);       /* 1/3 */
+    float r = z * p;
+    float ef = (float)e;
+    float two_s = sv + sv;
+    return fmaf(ef, LN2_HI_F, two_s + fmaf(two_s, r, ef * LN2_LO_F));
+}
+
+/* (w >> 8) + 1/2 over 2^24: exact in float, strictly inside (0, 1). */
+static float u24f(uint32_t w) { return ((float)(w >> 8) + 0.5f) * 0x1p-24f; }
 
 /* log(k!) for integer-valued k >= 0: table below 16, Stirling's series
  * (Bernoulli terms up to x^-7) above. */
@@ -586,11 +614,14 @@ int ctlo_simulate(const ctlo_model* m, uint32_t sim, const int32_t* X0, const fl
             double A0 = w.tree[1];
             if (A0 == 0.0) { finish_zero(m, &w, out, &cursor); T = m->tmax + (double)0.1f; break; }
             uint32_t step = n++;
+            /* one Philox block per two SSA steps: (w0,w1) for even steps,
+             * (w2,w3) for odd ones; 32-bit pick uniform, FP32 waiting time */
             uint32_t wd[4];
-            draw(m->seed, 0, TAG_SSA, step, sim, wd);
-            int r = descend(w.tree, P, u53(wd[0], wd[1]) * A0);
-            double dt = -ctlo_log(u53(wd[2], wd[3])) / A0;
-            tl = tl + dt;
+            draw(m->seed, 0, TAG_SSA, step >> 1, sim, wd);
+            uint32_t wa = (step & 1) ? wd[2] : wd[0], wb = (step & 1) ? wd[3] : wd[1];
+            int r = descend(w.tree, P, u32d(wa) * A0);
+            float dtf = -ctlo_logf(u24f(wb)) / (float)A0;
+            tl = tl + (double)dtf;
             while (cursor < (uint32_t)ns && T + tl > m->tvec[cursor]) {
                 for (int k = 0; k < so; k++) out[cursor * so + k] = (uint32_t)w.X[m->cs[k]];
                 cursor++;

@@ -95,6 +95,7 @@ int ctlo_run_batch(const ctlo_model* m, int n, uint32_t sim_base, const int32_t*
 /* Primitives exposed for known-answer and distribution tests. */
 void     ctlo_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 double   ctlo_log(double x);
+float    ctlo_logf(float x);
 double   ctlo_exp(double x);
 double   ctlo_logfact(double k);
 uint32_t ctlo_poisson(double lam, uint64_t seed, uint32_t sim, uint32_t step,

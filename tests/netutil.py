@@ -8,10 +8,13 @@ from cutauleaping_b200 import inputs
 def small_networks():
     """(name, Network) pairs covering orders 0-3, feed species, criticality."""
     nets = [("schlogl", inputs.schlogl(64, samples=40, t_end=2.0))]
-    for S, R, seed, t_end, x0 in [(4, 6, 3, 2.0, (5, 200)), (8, 12, 5, 2.0, (3, 300)),
-                                  (16, 32, 7, 1.0, (10, 2000)), (32, 64, 11, 0.5, (10, 10000))]:
-        net = inputs.synthetic(S, R, 48, seed=seed, t_end=t_end, samples=25, x0_range=x0)
-        nets.append((f"syn{S}x{R}", net))
+    for S, R, seed, t_end, x0, sigma in [(4, 6, 3, 2.0, (5, 200), 0.0), (8, 12, 5, 2.0, (3, 300), 0.5),
+                                         (16, 32, 7, 1.0, (10, 2000), 0.0),
+                                         (32, 64, 11, 0.5, (10, 10000), 0.5)]:
+        # sigma > 0: every simulation gets its own rate constants (per-row c path)
+        net = inputs.synthetic(S, R, 48, seed=seed, t_end=t_end, samples=25, x0_range=x0,
+                               perturb_sigma=sigma, perturb_seed=seed)
+        nets.append((f"syn{S}x{R}" + ("p" if sigma else ""), net))
     # immigration-death with a feed species and an order-3 reaction
     left = np.array([[0, 0, 0], [1, 0, 0], [3, 0, 0], [1, 0, 1]], np.int32)
     right = np.array([[1, 0, 0], [0, 0, 0], [2, 1, 0], [0, 1, 1]], np.int32)
