@@ -159,6 +159,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2, choices=[1, 2])
     ap.add_argument("--sims", type=int, default=None, help="simulations per GPU (default: config's)")
+    ap.add_argument("--group", type=int, default=0, help="lanes per simulation (0 = library choice)")
+    ap.add_argument("--threads", type=int, default=0, help="threads per block (0 = library choice)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     a = ap.parse_args()
@@ -195,7 +197,7 @@ def main():
     model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
     n = net.n
     sim_base = rank * n
-    cfg = ctl.run_cfg(seed=1, sim_base=sim_base, device=local,
+    cfg = ctl.run_cfg(seed=1, sim_base=sim_base, device=local, group=a.group, threads=a.threads,
                       uniform_rates=int(bool((net.c == net.c[0]).all())))
     li = model.launch_info(n, cfg)
     dev = torch.device("cuda", local)

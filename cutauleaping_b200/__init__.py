@@ -41,7 +41,8 @@ EXPORTS = [
     "ctl_model_dims_get", "ctl_model_hor", "ctl_rows_load", "ctl_run_cfg_default", "ctl_run",
     "ctl_run_device", "ctl_launch_query", "ctl_graph_create", "ctl_graph_launch", "ctl_graph_free",
     "ctl_write_dynamics", "ctl_print_dynamics", "ctl_target_load", "ctl_target_free",
-    "ctl_target_dims", "ctl_fitness",
+    "ctl_target_dims", "ctl_fitness", "ctl_fitness_device", "ctl_mlp_gemm", "ctl_mlp_nll_grad", "ctl_mlp_colsum",
+    "ctl_mlp_adam",
 ]
 
 
@@ -114,6 +115,8 @@ def lib():
         L.ctl_target_free.restype = None
         L.ctl_target_dims.argtypes = [P, P, P, P, P]
         L.ctl_fitness.argtypes = [P, P, C.POINTER(RunCfg), P, P]
+        L.ctl_fitness_device.argtypes = [P, C.c_uint32, C.c_uint32, P, P, C.c_uint32, C.c_uint32,
+                                         C.c_uint32, C.c_uint32, C.c_uint32, P, P]
         _lib = L
     return _lib
 

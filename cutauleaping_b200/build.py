@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-fmad=false", "-std=c++17",
                      "-Xcompiler", "-fPIC,-ffp-contract=off,-O3", f"-I{INCLUDE}"]
 
-LIB_SOURCES = ["ctl_sweep.cu", "ctl_host.cpp"]
+LIB_SOURCES = ["ctl_sweep.cu", "ctl_mlp.cu", "ctl_host.cpp"]
 CLI_SOURCES = ["ctl_cli.cpp"]
 
 

@@ -1477,6 +1477,22 @@ extern "C" void ctl_graph_free(ctl_graph* g) {
     delete g;
 }
 
+extern "C" ctl_status ctl_fitness_device(const uint32_t* d_samples, uint32_t ns, uint32_t s_out,
+                                         const uint32_t* d_target, const uint8_t* d_experiment,
+                                         uint32_t experiments, uint32_t repetitions, uint32_t threads,
+                                         uint32_t blocks, uint32_t p_rep, double* d_fitness, void* stream) {
+    if (!d_samples || !d_target || !d_experiment || !d_fitness || !threads || !blocks || !p_rep ||
+        blocks % p_rep || !ns || !s_out) {
+        set_error("ctl_fitness_device: invalid argument");
+        return CTL_ERR_ARG;
+    }
+    const uint32_t nsets = (uint32_t)(((uint64_t)threads * blocks) / p_rep);
+    dev::fitness_kernel<<<(nsets + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        d_samples, d_target, d_experiment, d_fitness, threads, nsets, p_rep, ns, s_out, experiments, repetitions);
+    CTL_CUDA(cudaGetLastError());
+    return CTL_OK;
+}
+
 extern "C" ctl_status ctl_fitness(ctl_model* m, const ctl_target* t, const ctl_run_cfg* cfg,
                                   const uint32_t* samples, double* fitness) {
     if (!m || !t || !cfg || !samples || !fitness) return CTL_ERR_ARG;

@@ -1,0 +1,237 @@
+"""Parameter estimation: plain-simulator search versus surrogate-screened search.
+
+The reference's fitness mode (kernel.cu:365-423) scores candidate parameter
+sets by simulating each of them p_rep times and comparing the ensemble mean
+with a target time series (calculateFitness, 2phase_n-tau-leaping.cu:
+3324-3408: sum over samples and species of |target - mean| / target, divided
+by samples x species).  The optimiser that proposes candidates lives outside
+the reference; here both searches use the same cross-entropy method (CEM) in
+log-parameter space:
+
+* plain:     every proposed candidate is simulated (n_rep simulations) and
+             scored with the reference fitness;
+* surrogate: every generation screens many candidates with the MLP
+             surrogate (cutauleaping_b200.surrogate), re-simulates only the
+             best 1% with the plain method and keeps the elite by that true
+             fitness; the plain method is the fallback and the judge.
+
+All simulation goes through the CUDA sweep (ctl_run_device) and the fitness
+through calculateFitness on the device (ctl_fitness_device).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import CtlError, Model, OK, lib, run_cfg
+from . import inputs
+from . import surrogate as sg
+
+
+@dataclass
+class FitProblem:
+    left: np.ndarray
+    right: np.ndarray
+    c_base: np.ndarray          # [R] rate constants (unknown ones replaced per candidate)
+    X0: np.ndarray              # [S]
+    tvec: np.ndarray            # [ns]
+    unknown: np.ndarray         # [8] reaction indices
+    theta_true: np.ndarray      # [8] log rate constants
+    log_lo: np.ndarray
+    log_hi: np.ndarray
+    target: np.ndarray          # [ns][S] uint32 ensemble mean (rounded), the fitting target
+    n_rep: int
+    model: Model = field(repr=False, default=None)
+
+    @property
+    def S(self):
+        return self.left.shape[1]
+
+
+def make_problem(S=32, R=64, *, net_seed=1, theta_seed=2, n_rep=512, samples=50, t_end=5.0,
+                 n_unknown=8, lo=1e-3, hi=1.0, sim_seed=77):
+    """A config-2-style random network with `n_unknown` rate constants
+    replaced by unknowns, their true values log-uniform in [lo, hi]; the
+    target is the mean of n_rep simulations at the true values."""
+    left, right, c, X0 = inputs.random_network(S, R, net_seed)
+    rng = np.random.default_rng(theta_seed)
+    order = left.sum(1)
+    cand = np.flatnonzero(order >= 1)
+    unknown = np.sort(rng.choice(cand, size=n_unknown, replace=False))
+    theta_true = rng.uniform(math.log(lo), math.log(hi), size=n_unknown)
+    tvec = t_end * np.arange(1, samples + 1) / samples
+    p = FitProblem(left, right, c, X0, tvec, unknown, theta_true, np.full(n_unknown, math.log(lo)),
+                   np.full(n_unknown, math.log(hi)), None, n_rep)
+    p.model = Model.create(left, right, None, tvec)
+    samples_ = simulate(p, theta_true[None, :], n_rep, seed=sim_seed, sim_base=1 << 30)
+    mean = samples_.reshape(n_rep, samples, S).astype(np.float64).mean(0)
+    p.target = np.rint(mean).astype(np.uint32)
+    return p
+
+
+def _rates(p: FitProblem, theta_log, n_rep, torch):
+    n = theta_log.shape[0]
+    c = torch.as_tensor(np.tile(p.c_base.astype(np.float32), (n, 1)), device="cuda")
+    c[:, torch.as_tensor(p.unknown, device="cuda")] = torch.exp(
+        torch.as_tensor(theta_log, dtype=torch.float32, device="cuda"))
+    return c.repeat_interleave(n_rep, dim=0).contiguous()
+
+
+def _sweep(p: FitProblem, theta_log, n_rep, seed, sim_base, torch):
+    """Simulate n_rep copies of every candidate; returns device samples
+    [n*n_rep][ns][S] (int32 view of the uint32 counts)."""
+    n = theta_log.shape[0]
+    N = n * n_rep
+    c = _rates(p, theta_log, n_rep, torch)
+    X0 = torch.as_tensor(np.tile(p.X0.astype(np.int32), (N, 1)), device="cuda")
+    out = torch.empty((N, len(p.tvec), p.S), dtype=torch.int32, device="cuda")
+    info = torch.empty((N, 40), dtype=torch.uint8, device="cuda")
+    cfg = run_cfg(seed=seed, sim_base=sim_base, max_steps=20_000_000)
+    p.model.run_device(N, X0.data_ptr(), c.data_ptr(), out.data_ptr(), info.data_ptr(),
+                       torch.cuda.current_stream().cuda_stream, cfg)
+    return out
+
+
+def simulate(p: FitProblem, theta_log, n_rep, *, seed, sim_base=0):
+    import torch
+    return _sweep(p, np.asarray(theta_log), n_rep, seed, sim_base, torch).cpu().numpy().view(np.uint32)
+
+
+def true_fitness(p: FitProblem, theta_log, *, seed, sim_base=0, chunk=256):
+    """Reference fitness of each candidate from n_rep simulations, on the device."""
+    import torch
+    L = lib()
+    theta_log = np.asarray(theta_log)
+    n = theta_log.shape[0]
+    tgt = torch.as_tensor(p.target.astype(np.uint32).view(np.int32).reshape(-1), device="cuda")
+    fit = np.empty(n)
+    for a in range(0, n, chunk):
+        th = theta_log[a:a + chunk]
+        k = th.shape[0]
+        out = _sweep(p, th, p.n_rep, seed, sim_base + a * p.n_rep, torch)
+        exp_id = torch.zeros(k, dtype=torch.uint8, device="cuda")
+        f = torch.zeros(k * p.n_rep, dtype=torch.float64, device="cuda")
+        st = L.ctl_fitness_device(C.c_void_p(out.data_ptr()), len(p.tvec), p.S, C.c_void_p(tgt.data_ptr()),
+                                  C.c_void_p(exp_id.data_ptr()), 1, 1, 1, k * p.n_rep, p.n_rep,
+                                  C.c_void_p(f.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if st != OK:
+            raise CtlError(st, "ctl_fitness_device")
+        fit[a:a + k] = f[:k].cpu().numpy()
+    return fit
+
+
+# ---------------------------------------------------------------------------
+# Surrogate training data, training, screening
+# ---------------------------------------------------------------------------
+
+def training_data(p: FitProblem, n_traj, *, seed=5, sim_seed=91):
+    """n_traj simulations, one per parameter set drawn from the prior box."""
+    import torch
+    rng = np.random.default_rng(seed)
+    theta = rng.uniform(p.log_lo, p.log_hi, size=(n_traj, len(p.unknown)))
+    out = _sweep(p, theta, 1, sim_seed, 1 << 31, torch)
+    return torch.as_tensor(theta, dtype=torch.float32, device="cuda"), out
+
+
+def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-3, seed=0, log=None):
+    """Fit the MLP to (theta, t) -> counts of single trajectories (Gaussian
+    NLL: the network learns the ensemble mean and log-variance)."""
+    import torch
+    n, ns, S = traj.shape
+    y = traj.to(torch.float32)
+    y_mean = y.mean(dim=(0, 1))
+    y_std = y.std(dim=(0, 1)).clamp_min(1.0)
+    sc = sg.Scaling(p.log_lo, p.log_hi, float(p.tvec[-1]), y_mean.cpu().numpy(), y_std.cpu().numpy())
+    tv = torch.as_tensor(p.tvec, dtype=torch.float32, device="cuda")
+    net = sg.MLP(S, seed=seed)
+    total = n * ns
+    steps = max(1, (epochs * total) // batch)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    hist = []
+    for it in range(steps):
+        idx = torch.randint(0, total, (batch,), device="cuda", generator=g)
+        si, ti = idx // ns, idx % ns
+        X = sg.make_inputs(theta[si], tv[ti], sc, torch)
+        tgt = (y[si, ti] - y_mean) / y_std
+        out = net.forward(X)
+        loss, dW, db = net.backward(out, tgt)
+        rate = lr * 0.5 * (1 + math.cos(math.pi * it / steps))
+        net.adam(dW, db, lr=rate)
+        if log is not None and (it % 200 == 0 or it == steps - 1):
+            hist.append((it, loss.item() / (batch * S)))
+    if log is not None:
+        log.extend(hist)
+    net.check_error_flag()
+    return net, sc
+
+
+def predicted_fitness(p: FitProblem, net, sc, theta_log, *, chunk=65536):
+    """Reference fitness computed from the surrogate's ensemble mean."""
+    import torch
+    theta_log = torch.as_tensor(np.asarray(theta_log), dtype=torch.float32, device="cuda")
+    n = theta_log.shape[0]
+    ns, S = len(p.tvec), p.S
+    tv = torch.as_tensor(p.tvec, dtype=torch.float32, device="cuda")
+    tgt = torch.as_tensor(p.target.astype(np.float64), device="cuda")
+    ym = torch.as_tensor(sc.y_mean, device="cuda", dtype=torch.float64)
+    ys = torch.as_tensor(sc.y_std, device="cuda", dtype=torch.float64)
+    fit = torch.empty(n, dtype=torch.float64, device="cuda")
+    per = max(1, chunk // ns)
+    for a in range(0, n, per):
+        th = theta_log[a:a + per]
+        k = th.shape[0]
+        rows = k * ns
+        pad = (-rows) % 128
+        X = sg.make_inputs(th.repeat_interleave(ns, 0), tv.repeat(k), sc, torch)
+        if pad:
+            X = torch.cat([X, torch.zeros(pad, X.shape[1], dtype=X.dtype, device="cuda")])
+        y = net.forward(X, keep=False)[:rows, :S].to(torch.float64)
+        mean = (y * ys + ym).view(k, ns, S)
+        d = (tgt - mean).abs()
+        d = torch.where(tgt != 0, d / tgt.clamp_min(1), d)
+        fit[a:a + k] = d.sum(dim=(1, 2)) / (ns * S)
+    return fit.cpu().numpy()
+
+
+# ---------------------------------------------------------------------------
+# Cross-entropy search
+# ---------------------------------------------------------------------------
+
+def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_frac=0.01, net=None,
+        sc=None, seed=0, sim_seed=1000, time_limit=None):
+    """Cross-entropy search in log-parameter space.  mode 'plain' simulates
+    every candidate; mode 'surrogate' screens `screen` candidates per
+    generation and simulates the best keep_frac of them.  Returns a list of
+    (wall seconds, simulations so far, best true fitness, best theta)."""
+    rng = np.random.default_rng(seed)
+    d = len(p.unknown)
+    mu = (p.log_lo + p.log_hi) / 2
+    sd = (p.log_hi - p.log_lo) / 2
+    best_f, best_t = math.inf, None
+    hist = []
+    sims = 0
+    t0 = time.perf_counter()
+    for gen in range(generations):
+        if mode == "plain":
+            cand = np.clip(rng.normal(mu, sd, size=(pop, d)), p.log_lo, p.log_hi)
+        else:
+            big = np.clip(rng.normal(mu, sd, size=(screen, d)), p.log_lo, p.log_hi)
+            pf = predicted_fitness(p, net, sc, big)
+            cand = big[np.argsort(pf)[: max(pop, int(keep_frac * screen))]]
+        f = true_fitness(p, cand, seed=sim_seed + gen, sim_base=0)
+        sims += len(cand) * p.n_rep
+        order = np.argsort(f)
+        if f[order[0]] < best_f:
+            best_f, best_t = float(f[order[0]]), cand[order[0]].copy()
+        ne = max(2, int(elite * len(cand)))
+        el = cand[order[:ne]]
+        mu = el.mean(0)
+        sd = np.maximum(el.std(0), 0.02 * (p.log_hi - p.log_lo))
+        hist.append((time.perf_counter() - t0, sims, best_f, best_t))
+        if time_limit is not None and time.perf_counter() - t0 > time_limit:
+            break
+    return hist

@@ -178,6 +178,54 @@ ctl_status ctl_target_dims(const ctl_target* t, uint32_t* repetitions, uint32_t*
 ctl_status ctl_fitness(ctl_model* m, const ctl_target* t, const ctl_run_cfg* cfg,
                        const uint32_t* samples, double* fitness);
 
+/* calculateFitness (tau.cu:3324-3408) on device buffers: samples
+ * [threads*blocks][ns][s_out], target [ns][experiments][repetitions][s_out],
+ * experiment id per parameter set (uint8), fitness [threads*blocks/p_rep]. */
+ctl_status ctl_fitness_device(const uint32_t* d_samples, uint32_t ns, uint32_t s_out,
+                              const uint32_t* d_target, const uint8_t* d_experiment,
+                              uint32_t experiments, uint32_t repetitions, uint32_t threads,
+                              uint32_t blocks, uint32_t p_rep, double* d_fitness, void* stream);
+
+/* ---- surrogate MLP kernels (fitness-mode screening) ---------------------- */
+/* No reference counterpart: the reference evaluates every candidate by full
+ * simulation (kernel.cu:365-423).  These are the tcgen05 kernels that train
+ * and run the screening surrogate; all pointers are device pointers. */
+enum {
+    CTL_EPI_ATOMIC_F32 = 0,  /* out_f32 += acc (split-K weight gradients)              */
+    CTL_EPI_BIAS_SILU = 1,   /* z = acc + bias -> out_f32; silu(z) -> out_bf, out_bfT  */
+    CTL_EPI_BIAS = 2,        /* out_f32 = acc + bias                                   */
+    CTL_EPI_SILU_GRAD = 3,   /* acc * silu'(z_in) -> out_bf, out_bfT                    */
+    CTL_EPI_F32 = 4          /* out_f32 = acc                                          */
+};
+typedef struct {
+    const void* A;          /* BF16 [M][lda], K contiguous */
+    const void* B;          /* BF16 [N][ldb], K contiguous */
+    int32_t lda, ldb, M, N, K;  /* M % 128 == 0, N % 16 == 0 (N <= 256 or N % 256 == 0), K % 64 == 0 */
+    int32_t epilogue;       /* CTL_EPI_* */
+    int32_t splits;         /* split-K factor (CTL_EPI_ATOMIC_F32), 0 or 1 = none */
+    const float* bias;      /* [N] */
+    const float* z_in;      /* [M][ldz] */
+    int32_t ldz;
+    float* out_f32;         /* [M][ldo] */
+    int32_t ldo;
+    void* out_bf;           /* BF16 [M][ldob] */
+    int32_t ldob;
+    void* out_bfT;          /* BF16 [N][ldobT], optional */
+    int32_t ldobT;
+    unsigned* err;          /* device word, bit 0 raised if a bounded wait timed out */
+} ctl_gemm_desc;
+/* C = A . B^T on the 5th-generation tensor cores (tcgen05.mma, TMEM). */
+ctl_status ctl_mlp_gemm(const ctl_gemm_desc* d, void* stream);
+/* Gaussian NLL gradient w.r.t. y = [mean | log-variance] (2S columns). */
+ctl_status ctl_mlp_nll_grad(const float* y, const float* target, int32_t B, int32_t S, void* dy,
+                            void* dyT, int32_t ldT, float* loss_sum, void* stream);
+/* Column sums of a BF16 [B][N] matrix, added to g[N]. */
+ctl_status ctl_mlp_colsum(const void* d, int32_t B, int32_t N, int32_t ld, float* g, void* stream);
+/* One Adam step on FP32 weights [rows][cols]; refreshes BF16 W and W^T. */
+ctl_status ctl_mlp_adam(float* w, const float* g, float* m1, float* m2, int32_t rows, int32_t cols,
+                        float lr, float beta1, float beta2, float eps, int32_t step, float weight_decay,
+                        void* w_bf16, void* wT_bf16, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
