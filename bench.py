@@ -43,16 +43,29 @@ METRIC = "sims/sec & reaction firings/sec on 1 B200 vs host build; surrogate-scr
 
 
 def workload(config: int, n: int | None = None):
+    """[(network, description)] segments of one benchmark step."""
     from cutauleaping_b200 import inputs
     if config == 1:
         net = inputs.schlogl(n or 4096)
-        desc = (f"Schlogl bistable model (schlogl.xml), {net.n} simulations, t_end=5, "
-                f"100 samples, eps=0.03, SSA factor 10, n_c=10")
-    else:
-        net = inputs.synthetic(64, 128, n or 65536, seed=0, t_end=10.0, samples=200)
-        desc = (f"synthetic mass-action network 64 species x 128 reactions (order 0-2, generator "
-                f"seed 0), {net.n} simulations, t_end=10, 200 samples, eps=0.03")
-    return net, desc
+        return [(net, f"Schlogl bistable model (schlogl.xml), {net.n} simulations, t_end=5, "
+                      f"100 samples, eps=0.03, SSA factor 10, n_c=10")]
+    if config == 3:
+        half = (n or 1 << 20) // 2
+        a = inputs.schlogl(half)
+        a.c = a.c * np.exp(0.5 * np.random.default_rng(30).standard_normal(a.c.shape))
+        b = inputs.synthetic(32, 64, half, seed=3, t_end=10.0, samples=200, perturb_sigma=0.5,
+                             perturb_seed=31)
+        return [(a, f"uneven batch part 1: Schlogl, {half} simulations with rates x exp(0.5 z)"),
+                (b, f"uneven batch part 2: synthetic 32x64 (generator seed 3), {half} simulations "
+                    f"with rates x exp(0.5 z), t_end=10, 200 samples")]
+    if config == 4:
+        net = inputs.synthetic(512, 1024, n or 16384, seed=0, t_end=20.0, samples=500,
+                               c_range=(1e-5, 1e-1), x0_range=(1, 100000))
+        return [(net, f"large sparse network 512 species x 1024 reactions (<= 4 nonzeros per "
+                      f"reaction, generator seed 0), {net.n} simulations, t_end=20, 500 samples")]
+    net = inputs.synthetic(64, 128, n or 65536, seed=0, t_end=10.0, samples=200)
+    return [(net, f"synthetic mass-action network 64 species x 128 reactions (order 0-2, generator "
+                  f"seed 0), {net.n} simulations, t_end=10, 200 samples, eps=0.03")]
 
 
 def op_count(net, info):
@@ -151,16 +164,32 @@ def cpu_reference(net, desc, steps, warmup, sample_s=10.0, threads=None):
         "cores": threads, "sample": f"{k} of the {net.n} simulations per step ({desc.split(',')[0]})"}
 
 
+def cpu_reference_segments(segs, steps, warmup):
+    """CPU port over every segment: sims/s of the whole step = total sims /
+    sum of per-segment times (each measured on a bounded sample)."""
+    tot_n, tot_t, tot_f, meta = 0, 0.0, 0.0, None
+    budget = 10.0 / len(segs)
+    samples = []
+    for net, desc in segs:
+        v, fv, meta = cpu_reference(net, desc, steps, warmup, sample_s=budget)
+        tot_n += net.n
+        tot_t += net.n / v
+        tot_f += fv * (net.n / v)
+        samples.append(meta["sample"])
+    return tot_n / tot_t, tot_f / tot_t, {"cores": meta["cores"], "sample": "; ".join(samples)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=2, choices=[1, 2])
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4])
     ap.add_argument("--sims", type=int, default=None, help="simulations per GPU (default: config's)")
     ap.add_argument("--group", type=int, default=0, help="lanes per simulation (0 = library choice)")
     ap.add_argument("--threads", type=int, default=0, help="threads per block (0 = library choice)")
+    ap.add_argument("--autotune", action="store_true", help="measure launch shapes before timing")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     a = ap.parse_args()
@@ -168,18 +197,20 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
-    net, desc = workload(a.config, a.sims)
+    segs = workload(a.config, a.sims)
+    desc = " + ".join(d for _, d in segs)
+    n_total = sum(net.n for net, _ in segs)
 
     if a.impl == "reference":
         if rank != 0:
             return
-        v, fv, meta = cpu_reference(net, desc, a.steps, a.warmup)
+        v, fv, meta = cpu_reference_segments(segs, a.steps, a.warmup)
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": "sims/s",
             "firings_per_s": fv, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32/f64/i32", "data": "synthetic",
-            "config": {"workload": desc, "sims": net.n},
+            "config": {"workload": desc, "sims": n_total},
             "cpu_baseline": {"value": v, "unit": "sims/s", "cores": meta["cores"], "kind": "port",
                              "sample": meta["sample"]},
             "e2e": {"value": v, "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -194,21 +225,25 @@ def main():
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-    model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
-    n = net.n
-    sim_base = rank * n
-    cfg = ctl.run_cfg(seed=1, sim_base=sim_base, device=local, group=a.group, threads=a.threads,
-                      uniform_rates=int(bool((net.c == net.c[0]).all())))
-    li = model.launch_info(n, cfg)
     dev = torch.device("cuda", local)
-    X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).to(dev)
-    c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).to(dev)
-    out = torch.empty((n, model.ns, model.s_out), dtype=torch.int32, device=dev)
-    info = torch.empty((n, 40), dtype=torch.uint8, device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.Stream(device=dev)
-    graph = model.graph(n, X0.data_ptr(), c.data_ptr(), out.data_ptr(), info.data_ptr(),
-                        stream.cuda_stream, cfg)
+    parts = []
+    for si, (net, _) in enumerate(segs):
+        model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+        n = net.n
+        cfg = ctl.run_cfg(seed=1 + si, sim_base=rank * n, device=local, group=a.group, threads=a.threads,
+                          uniform_rates=int(bool((net.c == net.c[0]).all())))
+        X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).to(dev)
+        c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).to(dev)
+        out = torch.empty((n, model.ns, model.s_out), dtype=torch.int32, device=dev)
+        info = torch.empty((n, 40), dtype=torch.uint8, device=dev)
+        if a.autotune:
+            model.autotune(n, X0.data_ptr(), c.data_ptr(), sample=min(n, max(4096, n // 16)), cfg=cfg)
+        li = model.launch_info(n, cfg)
+        graph = model.graph(n, X0.data_ptr(), c.data_ptr(), out.data_ptr(), info.data_ptr(),
+                            stream.cuda_stream, cfg)
+        parts.append(dict(net=net, model=model, cfg=cfg, X0=X0, c=c, out=out, info=info, li=li, graph=graph))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def barrier():
         if dist is not None:
@@ -217,7 +252,8 @@ def main():
     with torch.cuda.stream(stream):
         for _ in range(a.warmup):
             flush.fill_(1)
-            graph.launch(stream.cuda_stream)
+            for pt in parts:
+                pt["graph"].launch(stream.cuda_stream)
         stream.synchronize()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(a.steps)]
@@ -227,7 +263,8 @@ def main():
             for e0, e1 in ev:
                 flush.fill_(1)
                 e0.record(stream)
-                graph.launch(stream.cuda_stream)
+                for pt in parts:
+                    pt["graph"].launch(stream.cuda_stream)
                 e1.record(stream)
             stream.synchronize()
         torch.cuda.synchronize()
@@ -238,18 +275,25 @@ def main():
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    inf = info.cpu().numpy().view(ctl.INFO_DTYPE).reshape(-1)
-    fire = float(inf["firings"].sum())
+    fire, ops, abytes = 0.0, 0.0, 0.0
+    per_sim = {}
+    for pt in parts:
+        inf = pt["info"].cpu().numpy().view(ctl.INFO_DTYPE).reshape(-1)
+        fire += float(inf["firings"].sum())
+        ops += op_count(pt["net"], inf)
+        abytes += algorithmic_bytes(pt["net"]) * pt["net"].n
+        per_sim[pt["net"].name] = {"steps": float(inf["steps"].mean()), "leaps": float(inf["leaps"].mean()),
+                                   "ssa_steps": float(inf["ssa_steps"].mean()),
+                                   "status_ok": int((inf["status"] == 0).sum())}
     if dist is not None:
         f = torch.tensor([fire], dtype=torch.float64, device=dev)
         dist.all_reduce(f)
         fire = float(f.item())
-    value = world * n / (ms * 1e-3)
-    ops = op_count(net, inf)
-    abytes = algorithmic_bytes(net) * n
+    value = world * n_total / (ms * 1e-3)
     clocks = clk.summary()
     sm_mhz = clocks.get("sm_mhz") or 1965.0
-    issue_peak = li.sm_count * 128 * sm_mhz * 1e6  # FP32/INT32 lanes per SM x clock
+    li0 = parts[0]["li"]
+    issue_peak = li0.sm_count * 128 * sm_mhz * 1e6  # FP32/INT32 lanes per SM x clock
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -258,7 +302,7 @@ def main():
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     traffic = None
     tf = os.path.join(ROOT, "profiles", "sweep_traffic.txt")
-    if os.path.exists(tf) and a.config == 2 and n == 65536:
+    if os.path.exists(tf) and a.config == 2 and n_total == 65536:
         try:
             line = open(tf).read().split("#")[0]
             traffic = float(line.split(":")[1]) / 1e9  # GB per launch
@@ -267,19 +311,24 @@ def main():
 
     e2e = None
     if not a.no_e2e:
-        hX0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).pin_memory()
-        hc = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).pin_memory()
-        hout = torch.empty((n, model.ns, model.s_out), dtype=torch.int32).pin_memory()
-        hinfo = torch.empty((n, 40), dtype=torch.uint8).pin_memory()
         import ctypes as C
         L = ctl.lib()
+        host = []
+        for pt in parts:
+            net = pt["net"]
+            host.append(dict(
+                X0=torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).pin_memory(),
+                c=torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).pin_memory(),
+                out=torch.empty((net.n, pt["model"].ns, pt["model"].s_out), dtype=torch.int32).pin_memory(),
+                info=torch.empty((net.n, 40), dtype=torch.uint8).pin_memory()))
 
         def call():
-            st = L.ctl_run(model.handle, C.byref(cfg), n, C.c_void_p(hX0.data_ptr()),
-                           C.c_void_p(hc.data_ptr()), C.c_void_p(hout.data_ptr()),
-                           C.c_void_p(hinfo.data_ptr()))
-            if st not in (ctl.OK, ctl.ERR_STEP_LIMIT):
-                raise ctl.CtlError(st, "ctl_run")
+            for pt, h in zip(parts, host):
+                st = L.ctl_run(pt["model"].handle, C.byref(pt["cfg"]), pt["net"].n, C.c_void_p(h["X0"].data_ptr()),
+                               C.c_void_p(h["c"].data_ptr()), C.c_void_p(h["out"].data_ptr()),
+                               C.c_void_p(h["info"].data_ptr()))
+                if st not in (ctl.OK, ctl.ERR_STEP_LIMIT):
+                    raise ctl.CtlError(st, "ctl_run")
         call()
         barrier()
         et = []
@@ -292,16 +341,16 @@ def main():
             t = torch.tensor([e2e_s], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
-        e2e = {"value": world * n / e2e_s, "unit": "sims/s",
-               "h2d_bytes_per_step": int(hX0.numel() * 4 + hc.numel() * 4),
-               "d2h_bytes_per_step": int(hout.numel() * 4 + hinfo.numel()),
+        e2e = {"value": world * n_total / e2e_s, "unit": "sims/s",
+               "h2d_bytes_per_step": int(sum(h["X0"].numel() * 4 + h["c"].numel() * 4 for h in host)),
+               "d2h_bytes_per_step": int(sum(h["out"].numel() * 4 + h["info"].numel() for h in host)),
                "ms_per_step": e2e_s * 1e3, "timer": "host perf_counter around ctl_run"}
-        same = bool(np.array_equal(hout.numpy(), out.cpu().numpy()))
-        e2e["bit_identical_to_device_run"] = same
+        e2e["bit_identical_to_device_run"] = all(
+            bool(np.array_equal(h["out"].numpy(), pt["out"].cpu().numpy())) for pt, h in zip(parts, host))
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        v, fv, meta = cpu_reference(net, desc, 1, 0)
+        v, fv, meta = cpu_reference_segments(segs, 1, 0)
         cpu = {"value": v, "unit": "sims/s", "cores": meta["cores"], "kind": "port",
                "sample": meta["sample"], "firings_per_s": fv}
 
@@ -312,11 +361,13 @@ def main():
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32/f64/i32", "data": "synthetic",
-            "config": {"workload": desc, "sims_per_gpu": n, "seed": 1,
+            "config": {"workload": desc, "sims_per_gpu": n_total, "seed": 1,
                        "l2": "flushed between steps by a 256 MB device write",
-                       "launch": {"group": li.group, "threads": li.threads, "blocks": li.blocks,
-                                  "slots_per_block": li.slots_per_block, "smem_bytes": li.smem_bytes,
-                                  "regs": li.regs_per_thread, "blocks_per_sm": li.blocks_per_sm},
+                       "launch": [{"group": pt["li"].group, "threads": pt["li"].threads,
+                                   "blocks": pt["li"].blocks, "slots_per_block": pt["li"].slots_per_block,
+                                   "smem_bytes": pt["li"].smem_bytes, "regs": pt["li"].regs_per_thread,
+                                   "blocks_per_sm": pt["li"].blocks_per_sm} for pt in parts],
+                       "autotuned": bool(a.autotune),
                        "parallelism": f"dp{world} (independent simulations per rank)"},
             "roofline": {"bound": "hbm", "achieved": abytes / (ms * 1e-3) / 1e9,
                          "peak": hbm_peak, "unit": "GB/s",
@@ -328,19 +379,18 @@ def main():
             "roofline_issue": {"achieved": ops / (ms * 1e-3) / 1e12, "peak": issue_peak / 1e12,
                                "unit": "Tops/s", "frac": ops / (ms * 1e-3) / issue_peak,
                                "convention": "32-bit ops per SSA step / leap attempt (bench.op_count)",
-                               "peak_source": f"{li.sm_count} SMs x 128 FP32/INT32 lanes x median SM clock"},
-            "gpu_launches": a.steps,
+                               "peak_source": f"{li0.sm_count} SMs x 128 FP32/INT32 lanes x median SM clock"},
+            "gpu_launches": a.steps * len(parts),
             "clocks": clocks,
-            "per_sim": {"steps": float(inf["steps"].mean()), "leaps": float(inf["leaps"].mean()),
-                        "ssa_steps": float(inf["ssa_steps"].mean()),
-                        "status_ok": int((inf["status"] == 0).sum())},
+            "per_sim": per_sim,
         }
         if e2e is not None:
             line["e2e"] = e2e
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    del graph
+    for pt in parts:
+        del pt["graph"]
     if dist is not None:
         dist.destroy_process_group()
 

@@ -52,8 +52,8 @@ struct ctl_model {
     ctl::HostTables t;
     std::mutex mu;
     ctl::DeviceCopy dev[16];
-    // autotune cache: key = (device, n bucket) -> (group, threads)
-    struct Tuned { int device; uint32_t nbucket; int group, threads; };
+    // autotune cache: (device, log2 of the batch size, rate mode, flags) -> launch shape
+    struct Tuned { int device; uint32_t nbucket, uniform, flags; int group, threads, ssa_budget, dec_budget; };
     std::vector<Tuned> tuned;
 };
 

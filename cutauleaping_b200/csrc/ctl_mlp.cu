@@ -260,19 +260,19 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(Gemm p) {
 
 // ---- small kernels ------------------------------------------------------------------
 
-// Gaussian NLL per element: 0.5 (lv + (y - mu)^2 exp(-lv)), outputs y = [mu | lv]
-// (2*S columns), targets tgt [B][S].  Writes dY (BF16, [B][2S]) and its
-// transpose padded to 128 rows ([128][B], rows >= 2S zero), scaled by 1/(B*S),
-// and accumulates the loss sum.
-__global__ void nll_grad_kernel(const float* __restrict__ y, const float* __restrict__ tgt, int B, int S,
-                                __nv_bfloat16* __restrict__ dy, __nv_bfloat16* __restrict__ dyT, int ldT,
-                                float* __restrict__ loss) {
+// Gaussian NLL per element: 0.5 (lv + (y - mu)^2 exp(-lv)), outputs
+// y = [mu | lv | padding] (row stride ldy), targets tgt [B][S].  Writes dY
+// (BF16, row stride ldd; padding columns untouched) and its transpose
+// ([.][ldT], rows 0..2S-1), scaled by 1/(B*S), and accumulates the loss sum.
+__global__ void nll_grad_kernel(const float* __restrict__ y, int ldy, const float* __restrict__ tgt, int B,
+                                int S, __nv_bfloat16* __restrict__ dy, int ldd, __nv_bfloat16* __restrict__ dyT,
+                                int ldT, float* __restrict__ loss) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     float l = 0.0f;
     if (i < B * S) {
         const int b = i / S, s = i % S;
-        const float mu = y[(size_t)b * 2 * S + s];
-        float lv = y[(size_t)b * 2 * S + S + s];
+        const float mu = y[(size_t)b * ldy + s];
+        float lv = y[(size_t)b * ldy + S + s];
         lv = fminf(fmaxf(lv, -12.0f), 12.0f);
         const float iv = __expf(-lv);
         const float d = tgt[(size_t)b * S + s] - mu;
@@ -281,8 +281,8 @@ __global__ void nll_grad_kernel(const float* __restrict__ y, const float* __rest
         const float gmu = -d * iv * sc;
         const float glv = 0.5f * (1.0f - d * d * iv) * sc;
         const __nv_bfloat16 a = __float2bfloat16(gmu), c = __float2bfloat16(glv);
-        dy[(size_t)b * 2 * S + s] = a;
-        dy[(size_t)b * 2 * S + S + s] = c;
+        dy[(size_t)b * ldd + s] = a;
+        dy[(size_t)b * ldd + S + s] = c;
         dyT[(size_t)s * ldT + b] = a;
         dyT[(size_t)(S + s) * ldT + b] = c;
     }
@@ -375,12 +375,14 @@ extern "C" ctl_status ctl_mlp_gemm(const ctl_gemm_desc* d, void* stream) {
     return mlp_cuda(cudaGetLastError(), "gemm_kernel launch");
 }
 
-extern "C" ctl_status ctl_mlp_nll_grad(const float* y, const float* tgt, int32_t B, int32_t S, void* dy,
-                                       void* dyT, int32_t ldT, float* loss, void* stream) {
-    if (!y || !tgt || !dy || !dyT || !loss || B <= 0 || S <= 0 || 2 * S > 128 || ldT < B) return CTL_ERR_ARG;
+extern "C" ctl_status ctl_mlp_nll_grad(const float* y, int32_t ldy, const float* tgt, int32_t B, int32_t S,
+                                       void* dy, int32_t ldd, void* dyT, int32_t ldT, float* loss, void* stream) {
+    if (!y || !tgt || !dy || !dyT || !loss || B <= 0 || S <= 0 || 2 * S > 128 || ldT < B || ldy < 2 * S ||
+        ldd < 2 * S)
+        return CTL_ERR_ARG;
     const int n = B * S;
     mlp::nll_grad_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        y, tgt, B, S, static_cast<__nv_bfloat16*>(dy), static_cast<__nv_bfloat16*>(dyT), ldT, loss);
+        y, ldy, tgt, B, S, static_cast<__nv_bfloat16*>(dy), ldd, static_cast<__nv_bfloat16*>(dyT), ldT, loss);
     return mlp_cuda(cudaGetLastError(), "nll_grad_kernel launch");
 }
 

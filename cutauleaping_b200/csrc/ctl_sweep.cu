@@ -1104,6 +1104,7 @@ static dev::Model make_dev_model(const ctl_model* m, const DeviceCopy& d, uint32
 
 struct LaunchPlan {
     int G = 1, threads = 256, NS = 256, blocks = 1, blocks_per_sm = 1, sm_count = 1, regs = 0;
+    int ssa_budget = 0, dec_budget = 0;
     size_t smem = 0;
     dev::Layout lay{};
 };
@@ -1194,8 +1195,39 @@ static int heuristic_group(const HostTables& t) {
 
 // Launch shape for (model, cfg, n): group size, threads, slots and grid.
 // Small batches use smaller blocks so that every SM gets work.
-static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, LaunchPlan& pl) {
+static uint32_t n_bucket(uint32_t n) {
+    uint32_t b = 0;
+    while ((1u << b) < n && b < 31) b++;
+    return b;
+}
+
+// Autotuned shape for (device, batch bucket, rate mode, flags), if any.
+static bool find_tuned(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, ctl_model::Tuned& out) {
+    std::lock_guard<std::mutex> lk(m->mu);
+    for (const auto& e : m->tuned)
+        if (e.device == cfg->device && e.nbucket == n_bucket(n) && e.uniform == (uint32_t)(cfg->uniform_rates != 0) &&
+            e.flags == cfg->flags) {
+            out = e;
+            return true;
+        }
+    return false;
+}
+
+static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t n, LaunchPlan& pl) {
     const HostTables& t = m->t;
+    ctl_run_cfg tuned_cfg = *cfg_in;
+    if (cfg_in->group <= 0 && cfg_in->threads <= 0) {
+        ctl_model::Tuned e;
+        if (find_tuned(m, cfg_in, n, e)) {
+            tuned_cfg.group = e.group;
+            tuned_cfg.threads = e.threads;
+            if (tuned_cfg.ssa_budget <= 0) tuned_cfg.ssa_budget = e.ssa_budget;
+            if (tuned_cfg.dec_budget <= 0) tuned_cfg.dec_budget = e.dec_budget;
+        }
+    }
+    const ctl_run_cfg* cfg = &tuned_cfg;
+    pl.ssa_budget = cfg->ssa_budget;
+    pl.dec_budget = cfg->dec_budget;
     int G = cfg->group > 0 ? cfg->group : heuristic_group(t);
     if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32) {
         set_error("group must be one of 1, 2, 4, 8, 16, 32");
@@ -1265,8 +1297,8 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.sim_base = cfg->sim_base;
     run.n = n;
     run.uniform_c = cfg->uniform_rates != 0;
-    run.ssa_budget = cfg->ssa_budget > 0 ? (uint32_t)cfg->ssa_budget : 8u;
-    run.dec_budget = cfg->dec_budget > 0 ? (uint32_t)cfg->dec_budget : 2u;
+    run.ssa_budget = pl.ssa_budget > 0 ? (uint32_t)pl.ssa_budget : 8u;
+    run.dec_budget = pl.dec_budget > 0 ? (uint32_t)pl.dec_budget : 2u;
     run.X0 = dX0;
     run.c = dc;
     run.out = dout;
@@ -1423,6 +1455,94 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
             set_error("simulation " + std::to_string(i) + " ended with status " + std::to_string(info[i].status));
             return CTL_ERR_STEP_LIMIT;
         }
+    return CTL_OK;
+}
+
+// Measured autotuner: times candidate launch shapes on the first `sample`
+// simulations of the batch (results are identical for every shape, only the
+// time differs) -- group size first, then threads per block, then the
+// per-round budgets -- and caches the fastest for this (device, batch-size
+// bucket, rate mode, flags).
+extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* d_X0,
+                                   const float* d_c, uint32_t sample, ctl_launch_info* best) {
+    if (!m || !d_X0 || !d_c || n == 0) return CTL_ERR_ARG;
+    ctl_status st = check_cfg(cfg);
+    if (st != CTL_OK) return st;
+    const HostTables& t = m->t;
+    DeviceGuard dg(cfg->device);
+    DeviceCopy* d = nullptr;
+    if ((st = ensure_device(m, cfg->device, d)) != CTL_OK) return st;
+    const uint32_t k = sample == 0 || sample > n ? n : sample;
+    cudaStream_t s;
+    CTL_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    void *dout = nullptr, *dinf = nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaError_t e = cudaMallocAsync(&dout, (size_t)k * t.ns * t.s_out * 4, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dinf, (size_t)k * sizeof(ctl_sim_info), s);
+    auto time_shape = [&](int G, int threads, int sb, int db, float& ms) -> ctl_status {
+        ctl_run_cfg c = *cfg;
+        c.group = G;
+        c.threads = threads;
+        c.ssa_budget = sb;
+        c.dec_budget = db;
+        LaunchPlan pl;
+        ctl_status r = plan_launch(m, &c, k, pl);
+        if (r != CTL_OK) return r;
+        cudaEventRecord(e0, s);
+        r = enqueue_sweep(m, &c, k, d_X0, d_c, static_cast<uint32_t*>(dout), static_cast<ctl_sim_info*>(dinf), s, pl, *d);
+        cudaEventRecord(e1, s);
+        if (r != CTL_OK) return r;
+        if (cudaEventSynchronize(e1) != cudaSuccess) return CTL_ERR_CUDA;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return CTL_OK;
+    };
+    int bestG = heuristic_group(t), bestT = 256, bestS = 8, bestD = 2;
+    float best_ms = 3.4e38f;
+    if (e == cudaSuccess) {
+        for (int G = 1; G <= 32 && G <= t.P; G <<= 1) {  // 1. lanes per simulation
+            float ms;
+            if (time_shape(G, 256, 8, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestG = G; }
+        }
+        for (int th : {64, 128, 192}) {                   // 2. threads per block
+            float ms;
+            if (th % bestG == 0 && time_shape(bestG, th, 8, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestT = th; }
+        }
+        for (int sb : {2, 4, 16, 32}) {                    // 3. SSA steps per round
+            float ms;
+            if (time_shape(bestG, bestT, sb, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestS = sb; }
+        }
+        for (int db : {1, 4, 8}) {                         // 4. decisions per round
+            float ms;
+            if (time_shape(bestG, bestT, bestS, db, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestD = db; }
+        }
+    }
+    if (dout) cudaFreeAsync(dout, s);
+    if (dinf) cudaFreeAsync(dinf, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(e, "ctl_autotune");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "ctl_autotune (sweeps)");
+    {
+        std::lock_guard<std::mutex> lk(m->mu);
+        const uint32_t nb = n_bucket(n), uni = (uint32_t)(cfg->uniform_rates != 0);
+        bool found = false;
+        for (auto& x : m->tuned)
+            if (x.device == cfg->device && x.nbucket == nb && x.uniform == uni && x.flags == cfg->flags) {
+                x.group = bestG; x.threads = bestT; x.ssa_budget = bestS; x.dec_budget = bestD;
+                found = true;
+            }
+        if (!found) m->tuned.push_back({cfg->device, nb, uni, cfg->flags, bestG, bestT, bestS, bestD});
+    }
+    if (best) {
+        ctl_run_cfg c = *cfg;
+        c.group = 0;
+        c.threads = 0;
+        return ctl_launch_query(m, &c, n, best);
+    }
     return CTL_OK;
 }
 

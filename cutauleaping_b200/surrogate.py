@@ -43,7 +43,7 @@ def _bind():
     if not getattr(L, "_mlp_bound", False):
         P = C.c_void_p
         L.ctl_mlp_gemm.argtypes = [C.POINTER(GemmDesc), P]
-        L.ctl_mlp_nll_grad.argtypes = [P, P, C.c_int32, C.c_int32, P, P, C.c_int32, P, P]
+        L.ctl_mlp_nll_grad.argtypes = [P, C.c_int32, P, C.c_int32, C.c_int32, P, C.c_int32, P, C.c_int32, P, P]
         L.ctl_mlp_colsum.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, P, P]
         L.ctl_mlp_adam.argtypes = [P, P, P, P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float,
                                    C.c_float, C.c_int32, C.c_float, P, P, P]
@@ -106,13 +106,17 @@ class MLP:
         import torch
         self.torch = torch
         self.S = S
-        self.dims = [IN_PAD] + [HIDDEN] * LAYERS + [2 * S]
+        if 2 * S > 128:
+            raise ValueError("the surrogate predicts at most 64 species")
+        self.out_w = max(64, (2 * S + 63) // 64 * 64)  # output layer padded to a K tile
+        self.dims = [IN_PAD] + [HIDDEN] * LAYERS + [self.out_w]
         g = torch.Generator(device="cpu").manual_seed(seed)
         self.W, self.b, self.Wb, self.WbT, self.m, self.v, self.mb, self.vb = ([] for _ in range(8))
         for l in range(len(self.dims) - 1):
             fan_in, fan_out = (9 if l == 0 else self.dims[l]), self.dims[l + 1]
             w = torch.zeros(fan_out, self.dims[l])
-            w[:, :fan_in] = torch.randn(fan_out, fan_in, generator=g) * math.sqrt(1.0 / fan_in)
+            live = 2 * S if l == len(self.dims) - 2 else fan_out  # padded outputs stay zero
+            w[:live, :fan_in] = torch.randn(live, fan_in, generator=g) * math.sqrt(1.0 / fan_in)
             if l == len(self.dims) - 2:
                 w *= 0.1
             w = w.cuda()
@@ -154,7 +158,7 @@ class MLP:
             self.h.append(hn)
             self.hT.append(hT)
             h = hn
-        y = self._buf("y", (Bn, 2 * self.S), torch.float32)
+        y = self._buf("y", (Bn, self.out_w), torch.float32)
         gemm(h, self.Wb[LAYERS], epilogue=EPI_BIAS, out_f32=y, bias=self.b[LAYERS], err=self.err)
         return y
 
@@ -164,11 +168,13 @@ class MLP:
         torch = self.torch
         L = _bind()
         Bn, S = target.shape
-        dy = self._buf("dy", (Bn, 2 * S), torch.bfloat16)
+        dy = self._buf("dy", (Bn, self.out_w), torch.bfloat16)
+        dy.zero_()
         dyT = self._buf("dyT", (128, Bn), torch.bfloat16)
         dyT.zero_()
         loss = torch.zeros(1, device="cuda")
-        st = L.ctl_mlp_nll_grad(_ptr(y), _ptr(target), Bn, S, _ptr(dy), _ptr(dyT), Bn, _ptr(loss), _stream())
+        st = L.ctl_mlp_nll_grad(_ptr(y), y.stride(0), _ptr(target), Bn, S, _ptr(dy), dy.stride(0), _ptr(dyT), Bn,
+                                _ptr(loss), _stream())
         if st != OK:
             raise CtlError(st, "ctl_mlp_nll_grad")
         XT = self._buf("XT", (IN_PAD, Bn), torch.bfloat16)
@@ -179,7 +185,7 @@ class MLP:
         splits = max(1, min(64, Bn // 512))
         # output layer
         gemm(dyT, self.hT[LAYERS - 1], epilogue=EPI_ATOMIC_F32, out_f32=dW[LAYERS], splits=splits, err=self.err)
-        L.ctl_mlp_colsum(_ptr(dy), Bn, 2 * S, 2 * S, _ptr(db[LAYERS]), _stream())
+        L.ctl_mlp_colsum(_ptr(dy), Bn, self.out_w, self.out_w, _ptr(db[LAYERS]), _stream())
         g = dy
         for l in range(LAYERS - 1, -1, -1):
             dz = self._buf(f"dz{l}", (Bn, HIDDEN), torch.bfloat16)
@@ -189,7 +195,7 @@ class MLP:
             gemm(dzT, prevT, epilogue=EPI_ATOMIC_F32, out_f32=dW[l], splits=splits, err=self.err)
             L.ctl_mlp_colsum(_ptr(dz), Bn, HIDDEN, HIDDEN, _ptr(db[l]), _stream())
             g = dz
-        dW[LAYERS] = dW[LAYERS][: 2 * S].contiguous()
+        dW[LAYERS] = dW[LAYERS][: self.out_w].contiguous()
         return loss, dW, db
 
     def adam(self, dW, db, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, wd=0.0):

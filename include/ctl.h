@@ -148,6 +148,13 @@ ctl_status ctl_run_device(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
 ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
                             ctl_launch_info* li);
 
+/* Measured autotuner: times candidate shapes (lanes per simulation, threads
+ * per block, per-round budgets) on the first `sample` simulations of the
+ * batch on device buffers and caches the fastest; later calls with
+ * group == threads == 0 use it.  Never changes results. */
+ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* d_X0,
+                        const float* d_c, uint32_t sample, ctl_launch_info* best);
+
 /* One CUDA graph holding the whole sweep (queue reset + persistent kernel);
  * replay with ctl_graph_launch.  Buffers are bound at creation. */
 ctl_status ctl_graph_create(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
@@ -216,9 +223,10 @@ typedef struct {
 } ctl_gemm_desc;
 /* C = A . B^T on the 5th-generation tensor cores (tcgen05.mma, TMEM). */
 ctl_status ctl_mlp_gemm(const ctl_gemm_desc* d, void* stream);
-/* Gaussian NLL gradient w.r.t. y = [mean | log-variance] (2S columns). */
-ctl_status ctl_mlp_nll_grad(const float* y, const float* target, int32_t B, int32_t S, void* dy,
-                            void* dyT, int32_t ldT, float* loss_sum, void* stream);
+/* Gaussian NLL gradient w.r.t. y = [mean | log-variance | padding] (row
+ * stride ldy >= 2S); dy BF16 [B][ldd], dyT BF16 [2S..][ldT]. */
+ctl_status ctl_mlp_nll_grad(const float* y, int32_t ldy, const float* target, int32_t B, int32_t S,
+                            void* dy, int32_t ldd, void* dyT, int32_t ldT, float* loss_sum, void* stream);
 /* Column sums of a BF16 [B][N] matrix, added to g[N]. */
 ctl_status ctl_mlp_colsum(const void* d, int32_t B, int32_t N, int32_t ld, float* g, void* stream);
 /* One Adam step on FP32 weights [rows][cols]; refreshes BF16 W and W^T. */

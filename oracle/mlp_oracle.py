@@ -41,13 +41,16 @@ def forward(X, W, b):
 
 
 def nll_grad(y, tgt):
+    """y = [mu | log var | zero padding]; the padding columns get zero gradient."""
     Bn, S = tgt.shape
-    mu, lv = y[:, :S], np.clip(y[:, S:], -12.0, 12.0)
+    mu, lv = y[:, :S], np.clip(y[:, S:2 * S], -12.0, 12.0)
     iv = np.exp(-lv)
     d = tgt - mu
     loss = float((0.5 * (lv + d * d * iv)).sum())
     sc = 1.0 / (Bn * S)
-    dy = np.concatenate([-d * iv * sc, 0.5 * (1.0 - d * d * iv) * sc], axis=1).astype(np.float32)
+    dy = np.zeros_like(y)
+    dy[:, :S] = -d * iv * sc
+    dy[:, S:2 * S] = 0.5 * (1.0 - d * d * iv) * sc
     return loss, bf16(dy)
 
 

@@ -97,6 +97,7 @@ def test_mlp_gradients_match_cpu_oracle():
     b = [x.cpu().numpy() for x in net.b]
     l_o, dW_o, db_o, y_o = mo.backward(X, W, b, tgt)
     assert np.allclose(y.cpu().numpy(), y_o, rtol=2e-2, atol=2e-3)
+    assert net.out_w == 64 and np.all(W[-1][2 * S:] == 0)
     assert abs(loss.item() - l_o) / abs(l_o) < 1e-3
     for l in range(len(W)):
         g, o = dW[l].cpu().numpy(), dW_o[l]
