@@ -179,13 +179,69 @@ def cpu_reference_segments(segs, steps, warmup):
     return tot_n / tot_t, tot_f / tot_t, {"cores": meta["cores"], "sample": "; ".join(samples)}
 
 
+def bench_config5(a):
+    """Surrogate-screened parameter estimation against plain-simulator search.
+
+    Both searches run the same cross-entropy method (cutauleaping_b200.fitsearch);
+    the surrogate search pays for its training data and training inside its
+    wall time.  fits/s = 1 / wall seconds to reach the common fitness level
+    (the worse of the two final best fitnesses, +2%)."""
+    import torch
+    from cutauleaping_b200 import fitsearch as fs
+    full = a.full
+    n_rep = 512 if full else 64
+    n_traj = (1 << 20) if full else (1 << 16)
+    screen = 1_000_000 if full else 100_000
+    gens, pop = (8, 10_000) if full else (6, 1000)
+    p = fs.make_problem(n_rep=n_rep, samples=50, t_end=5.0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = fs.cem(p, mode="plain", generations=gens, pop=pop, seed=1)
+    t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    theta, traj = fs.training_data(p, n_traj)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    net, sc = fs.train_surrogate(p, theta, traj, epochs=2, batch=16384)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0 - t_data
+    surr = fs.cem(p, mode="surrogate", generations=gens, pop=pop, screen=screen, keep_frac=0.01, net=net,
+                  sc=sc, seed=1)
+    pre = t_data + t_train
+    f_star = max(plain[-1][2], surr[-1][2]) * 1.02
+
+    def reach(hist, offset):
+        for wall, sims, f, _ in hist:
+            if f <= f_star:
+                return offset + wall, sims
+        return offset + hist[-1][0], hist[-1][1]
+    tp, sp = reach(plain, 0.0)
+    ts, ss = reach(surr, pre)
+    truth = fs.true_fitness(p, p.theta_true[None, :], seed=4242)[0]
+    print(json.dumps({
+        "metric": METRIC, "config": {"workload": "surrogate-screened parameter estimation: 32x64 network "
+                                                 "(generator seed 1), 8 unknown rate constants, target = mean "
+                                                 f"of {n_rep} simulations at 50 instants", "full_size": full,
+                                     "n_rep": n_rep, "training_trajectories": n_traj, "screened_per_gen": screen,
+                                     "resimulated_per_gen": pop, "generations": gens},
+        "value": 1.0 / ts, "unit": "fits/s (surrogate-screened)", "plain_fits_per_s": 1.0 / tp,
+        "speedup_vs_plain": tp / ts, "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+        "final_fitness": {"plain": plain[-1][2], "surrogate": surr[-1][2], "true_parameters": float(truth),
+                          "common_level": f_star},
+        "time_s": {"plain_to_level": tp, "surrogate_to_level": ts, "surrogate_data": t_data,
+                   "surrogate_training": t_train, "plain_total": t_plain},
+        "simulations_to_level": {"plain": sp, "surrogate": ss},
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4])
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5])
+    ap.add_argument("--full", action="store_true", help="config 5 at the configured sizes")
     ap.add_argument("--sims", type=int, default=None, help="simulations per GPU (default: config's)")
     ap.add_argument("--group", type=int, default=0, help="lanes per simulation (0 = library choice)")
     ap.add_argument("--threads", type=int, default=0, help="threads per block (0 = library choice)")
@@ -197,6 +253,13 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if a.config == 5:
+        if rank == 0 and a.impl == "ours":
+            bench_config5(a)
+        elif rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "config 5 is a search benchmark; its "
+                              "plain-simulator arm is reported inside the config-5 line"}), flush=True)
+        return
     segs = workload(a.config, a.sims)
     desc = " + ".join(d for _, d in segs)
     n_total = sum(net.n for net, _ in segs)
@@ -238,7 +301,8 @@ def main():
         out = torch.empty((n, model.ns, model.s_out), dtype=torch.int32, device=dev)
         info = torch.empty((n, 40), dtype=torch.uint8, device=dev)
         if a.autotune:
-            model.autotune(n, X0.data_ptr(), c.data_ptr(), sample=min(n, max(4096, n // 16)), cfg=cfg)
+            # the sample must fill the GPU like the full batch does: a quarter of it, >= 16384
+            model.autotune(n, X0.data_ptr(), c.data_ptr(), sample=min(n, max(16384, n // 4)), cfg=cfg)
         li = model.launch_info(n, cfg)
         graph = model.graph(n, X0.data_ptr(), c.data_ptr(), out.data_ptr(), info.data_ptr(),
                             stream.cuda_stream, cfg)

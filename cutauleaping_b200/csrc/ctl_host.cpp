@@ -82,6 +82,19 @@ ctl_status build_tables(int S, int R, const int32_t* left, const int32_t* right,
             if (left[(size_t)r * S + s] > 0) t.reac_ent.push_back(pack((uint32_t)s, left[(size_t)r * S + s]));
         t.reac_off.push_back((uint32_t)t.reac_ent.size());
     }
+    // Packed reactant descriptors: the common case of at most two reactant
+    // entries with coefficients 1 or 2 needs one table load per propensity.
+    t.reac_desc.assign((size_t)2 * R, 0u);
+    for (int r = 0; r < R; r++) {
+        const uint32_t e0 = t.reac_off[r], e1 = t.reac_off[r + 1];
+        bool simple = e1 - e0 <= 2;
+        for (uint32_t e = e0; e < e1; e++) simple = simple && (t.reac_ent[e] & 0xffu) <= 2;
+        if (!simple) {
+            t.reac_desc[2 * r] = 0xffffffffu;
+            continue;
+        }
+        for (uint32_t e = e0; e < e1; e++) t.reac_desc[2 * r + (e - e0)] = t.reac_ent[e];
+    }
     // V species-major = RAV (tau.cu:314-326); F species-major and reaction-major
     t.vs_off.push_back(0);
     t.fs_off.push_back(0);

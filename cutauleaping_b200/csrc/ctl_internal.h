@@ -21,6 +21,8 @@ inline uint32_t pack(uint32_t idx, int coef) { return (idx << 8) | (uint32_t)(ui
 struct HostTables {
     int S = 0, R = 0, P = 2, logP = 1, ns = 0, s_out = 0;
     std::vector<uint32_t> reac_off, reac_ent;  // reactants (left > 0), r-major: s<<8|st
+    std::vector<uint32_t> reac_desc;           // [2R]: up to two reactant entries (s<<8|st, 0 = none);
+                                               // 0xffffffff in slot 0 = use the general list
     std::vector<uint32_t> vs_off, vs_ent;      // V = right-left, species-major: r<<8|v
     std::vector<uint32_t> fs_off, fs_ent;      // F (feed-masked V), species-major: r<<8|f
     std::vector<uint32_t> fr_off, fr_ent;      // F, reaction-major: s<<8|f
@@ -39,6 +41,7 @@ struct DeviceCopy {
     size_t off_reac_off = 0, off_reac_ent = 0, off_vs_off = 0, off_vs_ent = 0;
     size_t off_fs_off = 0, off_fs_ent = 0, off_fr_off = 0, off_fr_ent = 0;
     size_t off_dep_off = 0, off_dep_ent = 0, off_hor = 0, off_hort = 0, off_tvec = 0, off_cs = 0;
+    size_t off_reac_desc = 0;
 };
 
 void set_error(const std::string& msg);

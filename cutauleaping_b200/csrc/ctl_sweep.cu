@@ -53,6 +53,7 @@ struct Model {
     int S, R, P, logP, ns, s_out;
     const uint32_t* __restrict__ reac_off;
     const uint32_t* __restrict__ reac_ent;
+    const uint2* __restrict__ reac_desc;  // [R] packed reactants, x == 0xffffffff: general list
     const uint32_t* __restrict__ v_off;  // V or F species-major (quirk Q5)
     const uint32_t* __restrict__ v_ent;
     const uint32_t* __restrict__ fs_off;
@@ -341,9 +342,35 @@ struct Slot {
     __device__ __forceinline__ float& cf(int i) const { return c[i * cst]; }
 };
 
-// Mass-action propensity in FP32 (CalculatePropensity, tau.cu:1443-1470).
+// One reactant factor: X for coefficient 1, 0.5 X (X-1) for 2.
+__device__ __forceinline__ float react_factor(int32_t x, uint32_t st) {
+    const float hx = (float)x;
+    return st == 1u ? hx : (0.5f * hx) * (hx - 1.0f);
+}
+
+// Mass-action propensity in FP32 (CalculatePropensity, tau.cu:1443-1470):
+// c times, per reactant entry in species order, X (coefficient 1),
+// 0.5 X (X-1) (coefficient 2) or the product of (X-e+1)/e (higher); zero when
+// a reactant count is below its coefficient.  Reactions with at most two
+// entries of coefficient <= 2 read one packed descriptor.
 __device__ __forceinline__ float prop(const Model& m, const Slot& sl, int r) {
     float v = sl.cf(r);
+    const uint2 d = m.reac_desc[r];
+    if (d.x != 0xffffffffu) {
+        if (d.x) {
+            const int32_t x = sl.x((int)(d.x >> 8));
+            const uint32_t st = d.x & 0xffu;
+            if (x < (int32_t)st) return 0.0f;
+            v = v * react_factor(x, st);
+        }
+        if (d.y) {
+            const int32_t x = sl.x((int)(d.y >> 8));
+            const uint32_t st = d.y & 0xffu;
+            if (x < (int32_t)st) return 0.0f;
+            v = v * react_factor(x, st);
+        }
+        return v;
+    }
     const uint32_t e1 = m.reac_off[r + 1];
     for (uint32_t e = m.reac_off[r]; e < e1; e++) {
         const uint32_t ent = m.reac_ent[e];
@@ -925,8 +952,16 @@ __global__ void __launch_bounds__(256) sweep_kernel(Model m, Run run, Layout lay
         __syncthreads();
         const uint32_t nssa = s_cnt[0], ndec = s_cnt[1];
         if (nssa + ndec == 0u) break;
-        for (uint32_t k = (uint32_t)gi; k < nssa + ndec; k += (uint32_t)NS) {
-            const bool is_ssa = k < nssa;
+        // At most one list entry per group and round (nssa + ndec <= NS).
+        // The groups of a warp that work in the same phase step in lockstep:
+        // before every step they agree (__any_sync over that phase's lanes)
+        // whether anyone still has work, so their instruction streams merge.
+        const uint32_t k = (uint32_t)gi;
+        const bool has_item = k < nssa + ndec;
+        const bool is_ssa = k < nssa;
+        const uint32_t ssa_mask = __ballot_sync(0xffffffffu, is_ssa);
+        const uint32_t dec_mask = __ballot_sync(0xffffffffu, has_item && !is_ssa);
+        if (has_item) {
             const int j = (int)(is_ssa ? list[k] : list[NS - 1 - (int)(k - nssa)]);
             const Slot sl = slot_of<G>(smem, lay, j, NS, uni);
             Sim st;
@@ -934,11 +969,17 @@ __global__ void __launch_bounds__(256) sweep_kernel(Model m, Run run, Layout lay
             uint32_t* out = run.out + (size_t)st.sim * sim_stride;
             int res = CONT;
             if (is_ssa) {
-                for (uint32_t b = 0; b < run.ssa_budget && res == CONT && st.in_ssa; b++)
-                    res = ssa_step<G>(g, m, run, sl, st, out);
+                for (uint32_t b = 0; b < run.ssa_budget; b++) {
+                    const bool act = res == CONT && st.in_ssa;
+                    if (!__any_sync(ssa_mask, act)) break;
+                    if (act) res = ssa_step<G>(g, m, run, sl, st, out);
+                }
             } else {
-                for (uint32_t b = 0; b < run.dec_budget && res == CONT && !st.in_ssa; b++)
-                    res = decide_step<G>(g, m, run, sl, st, out);
+                for (uint32_t b = 0; b < run.dec_budget; b++) {
+                    const bool act = res == CONT && !st.in_ssa;
+                    if (!__any_sync(dec_mask, act)) break;
+                    if (act) res = decide_step<G>(g, m, run, sl, st, out);
+                }
             }
             if (res == DONE) {
                 finish_sim<G>(g, m, run, st, out);
@@ -1020,6 +1061,7 @@ static ctl_status ensure_device(ctl_model* m, int device, DeviceCopy*& out) {
     };
     d.off_reac_off = place(t.reac_off.size() * 4);
     d.off_reac_ent = place(std::max<size_t>(1, t.reac_ent.size()) * 4);
+    d.off_reac_desc = place(t.reac_desc.size() * 4);
     d.off_vs_off = place(t.vs_off.size() * 4);
     d.off_vs_ent = place(std::max<size_t>(1, t.vs_ent.size()) * 4);
     d.off_fs_off = place(t.fs_off.size() * 4);
@@ -1040,6 +1082,7 @@ static ctl_status ensure_device(ctl_model* m, int device, DeviceCopy*& out) {
     };
     put(d.off_reac_off, t.reac_off.data(), t.reac_off.size() * 4);
     put(d.off_reac_ent, t.reac_ent.data(), t.reac_ent.size() * 4);
+    put(d.off_reac_desc, t.reac_desc.data(), t.reac_desc.size() * 4);
     put(d.off_vs_off, t.vs_off.data(), t.vs_off.size() * 4);
     put(d.off_vs_ent, t.vs_ent.data(), t.vs_ent.size() * 4);
     put(d.off_fs_off, t.fs_off.data(), t.fs_off.size() * 4);
@@ -1084,6 +1127,7 @@ static dev::Model make_dev_model(const ctl_model* m, const DeviceCopy& d, uint32
     dm.S = t.S; dm.R = t.R; dm.P = t.P; dm.logP = t.logP; dm.ns = t.ns; dm.s_out = t.s_out;
     dm.reac_off = reinterpret_cast<const uint32_t*>(P(d.off_reac_off));
     dm.reac_ent = reinterpret_cast<const uint32_t*>(P(d.off_reac_ent));
+    dm.reac_desc = reinterpret_cast<const uint2*>(P(d.off_reac_desc));
     const bool q5off = (flags & dev::F_Q5_OFF) != 0;
     dm.v_off = reinterpret_cast<const uint32_t*>(P(q5off ? d.off_fs_off : d.off_vs_off));
     dm.v_ent = reinterpret_cast<const uint32_t*>(P(q5off ? d.off_fs_ent : d.off_vs_ent));
