@@ -39,7 +39,7 @@ INFO_DTYPE = np.dtype([
 EXPORTS = [
     "ctl_status_str", "ctl_last_error", "ctl_model_load", "ctl_model_create", "ctl_model_free",
     "ctl_model_dims_get", "ctl_model_hor", "ctl_rows_load", "ctl_run_cfg_default", "ctl_run",
-    "ctl_run_device", "ctl_launch_query", "ctl_autotune", "ctl_graph_create", "ctl_graph_launch", "ctl_graph_free",
+    "ctl_run_device", "ctl_run_device_noalloc", "ctl_launch_query", "ctl_autotune", "ctl_graph_create", "ctl_graph_launch", "ctl_graph_free",
     "ctl_write_dynamics", "ctl_print_dynamics", "ctl_target_load", "ctl_target_free",
     "ctl_target_dims", "ctl_fitness", "ctl_fitness_device", "ctl_mlp_gemm", "ctl_mlp_nll_grad", "ctl_mlp_colsum",
     "ctl_mlp_adam",
@@ -104,6 +104,7 @@ def lib():
         L.ctl_run.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, P, P]
         L.ctl_run_device.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, P, P, P]
         L.ctl_launch_query.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, C.POINTER(LaunchInfo)]
+        L.ctl_run_device_noalloc.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, P, P, P]
         L.ctl_autotune.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, C.c_uint32, C.POINTER(LaunchInfo)]
         L.ctl_graph_create.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, P, P, P, C.POINTER(P)]
         L.ctl_graph_launch.argtypes = [P, P]

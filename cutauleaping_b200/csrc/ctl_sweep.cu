@@ -1698,3 +1698,118 @@ extern "C" ctl_status ctl_fitness(ctl_model* m, const ctl_target* t, const ctl_r
     if (e2 != cudaSuccess) return cuda_fail(e2, "ctl_fitness (kernel)");
     return CTL_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free sweep
+// ---------------------------------------------------------------------------
+//
+// Some callers cannot call cudaMalloc: an application that hands out device
+// memory only through its own pool allocator, a host that has already sized
+// and locked its device memory budget, or a library layer that must not grow
+// device memory behind its caller's back.  ctl_run_device needs device memory
+// of its own for the model tables and the work-queue ticket, which it
+// allocates on first use per device.  ctl_run_device_noalloc keeps both in
+// the fixed array below instead and allocates nothing.
+
+namespace ctl {
+
+// Holds the work-queue ticket (first 256 bytes) and the model tables of the
+// call in progress.  It lives in every device that loads this library, for
+// as long as the library stays loaded.
+constexpr size_t NOALLOC_BYTES = (size_t)1 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_base[16];  // device address of g_noalloc_scratch, per device
+
+}  // namespace ctl
+
+extern "C" ctl_status ctl_run_device_noalloc(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
+                                             const int32_t* d_X0, const float* d_c, uint32_t* d_samples,
+                                             ctl_sim_info* d_info, void* stream) {
+    if (!m) return CTL_ERR_ARG;
+    ctl_status st = check_cfg(cfg);
+    if (st != CTL_OK) return st;
+    if (cfg->device < 0 || cfg->device >= 16) {
+        set_error("device ordinal out of range");
+        return CTL_ERR_ARG;
+    }
+    const HostTables& t = m->t;
+    // Same table layout as the allocating path, after a 256-byte ticket area.
+    DeviceCopy d;
+    size_t off = 256;
+    auto place = [&](size_t bytes) {
+        size_t o = off;
+        off = align16(off + bytes);
+        return o;
+    };
+    d.off_reac_off = place(t.reac_off.size() * 4);
+    d.off_reac_ent = place(std::max<size_t>(1, t.reac_ent.size()) * 4);
+    d.off_reac_desc = place(t.reac_desc.size() * 4);
+    d.off_vs_off = place(t.vs_off.size() * 4);
+    d.off_vs_ent = place(std::max<size_t>(1, t.vs_ent.size()) * 4);
+    d.off_fs_off = place(t.fs_off.size() * 4);
+    d.off_fs_ent = place(std::max<size_t>(1, t.fs_ent.size()) * 4);
+    d.off_fr_off = place(t.fr_off.size() * 4);
+    d.off_fr_ent = place(std::max<size_t>(1, t.fr_ent.size()) * 4);
+    d.off_dep_off = place(t.dep_off.size() * 4);
+    d.off_dep_ent = place(std::max<size_t>(1, t.dep_ent.size()) * 4);
+    d.off_hor = place(t.hor.size());
+    d.off_hort = place(t.hort.size());
+    d.off_tvec = place(t.tvec.size() * 8);
+    d.off_cs = place(t.cs.size() * 4);
+    if (off > NOALLOC_BYTES) {
+        set_error("ctl_run_device_noalloc: the model tables need " + std::to_string(off) +
+                  " bytes, the allocation-free path holds at most " + std::to_string(NOALLOC_BYTES) +
+                  " (1 MiB); use ctl_run_device");
+        return CTL_ERR_SHAPE;
+    }
+    if (n == 0) return CTL_OK;
+    if (!d_X0 || !d_c || !d_samples || !d_info) {
+        set_error("null device buffer");
+        return CTL_ERR_ARG;
+    }
+    DeviceGuard dg(cfg->device);
+    void* base = nullptr;
+    {
+        // Set-up, once per device with that device current: the host-side
+        // name of the array is not a device address; ask for its address.
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_base[cfg->device]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+            g_noalloc_base[cfg->device] = p;
+        }
+        base = g_noalloc_base[cfg->device];
+    }
+    d.device = cfg->device;
+    d.buf = base;
+    d.bytes = off;
+    d.ctrl = static_cast<uint32_t*>(base);  // ticket: cleared by enqueue_sweep before the launch
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char* b = static_cast<unsigned char*>(base);
+    auto put = [&](size_t o, const void* src, size_t bytes) -> cudaError_t {
+        return bytes ? cudaMemcpyAsync(b + o, src, bytes, cudaMemcpyHostToDevice, s) : cudaSuccess;
+    };
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = put(d.off_reac_off, t.reac_off.data(), t.reac_off.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_reac_ent, t.reac_ent.data(), t.reac_ent.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_reac_desc, t.reac_desc.data(), t.reac_desc.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_vs_off, t.vs_off.data(), t.vs_off.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_vs_ent, t.vs_ent.data(), t.vs_ent.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_fs_off, t.fs_off.data(), t.fs_off.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_fs_ent, t.fs_ent.data(), t.fs_ent.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_fr_off, t.fr_off.data(), t.fr_off.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_fr_ent, t.fr_ent.data(), t.fr_ent.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_dep_off, t.dep_off.data(), t.dep_off.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_dep_ent, t.dep_ent.data(), t.dep_ent.size() * 4);
+    if (e == cudaSuccess) e = put(d.off_hor, t.hor.data(), t.hor.size());
+    if (e == cudaSuccess) e = put(d.off_hort, t.hort.data(), t.hort.size());
+    if (e == cudaSuccess) e = put(d.off_tvec, t.tvec.data(), t.tvec.size() * 8);
+    if (e == cudaSuccess) e = put(d.off_cs, t.cs.data(), t.cs.size() * 4);
+    if (e != cudaSuccess) return cuda_fail(e, "ctl_run_device_noalloc (tables)");
+    LaunchPlan pl;
+    if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;
+    return enqueue_sweep(m, cfg, n, d_X0, d_c, d_samples, d_info, s, pl, d);
+}

@@ -148,6 +148,22 @@ ctl_status ctl_run_device(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
 ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
                             ctl_launch_info* li);
 
+/* The same sweep as ctl_run_device, for callers that cannot allocate device
+ * memory (an application whose device memory comes only from its own pool,
+ * a host that has fixed its device-memory budget, a layer that must not grow
+ * memory behind its caller).  No counterpart in the reference.  The model
+ * tables and the work-queue ticket live in a fixed 1 MiB array inside the
+ * library instead of a cudaMalloc'd copy; models whose tables need more are
+ * rejected with CTL_ERR_SHAPE.  The call allocates nothing: no cudaMalloc,
+ * no cudaFree, no allocating library routine.  The first call on a device
+ * looks up the array's device address (make it before any stream capture).
+ * Every call reuses the same array and leaves its contents behind, so calls
+ * whose work overlaps on the GPU (other streams, other threads) race: issue
+ * them one after another. */
+ctl_status ctl_run_device_noalloc(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
+                                  const int32_t* d_X0, const float* d_c, uint32_t* d_samples,
+                                  ctl_sim_info* d_info, void* stream);
+
 /* Measured autotuner: times candidate shapes (lanes per simulation, threads
  * per block, per-round budgets) on the first `sample` simulations of the
  * batch on device buffers and caches the fastest; later calls with
