@@ -182,22 +182,30 @@ def cpu_reference_segments(segs, steps, warmup):
 def bench_config5(a):
     """Surrogate-screened parameter estimation against plain-simulator search.
 
-    Both searches run the same cross-entropy method (cutauleaping_b200.fitsearch);
-    the surrogate search pays for its training data and training inside its
-    wall time.  fits/s = 1 / wall seconds to reach the common fitness level
-    (the worse of the two final best fitnesses, +2%)."""
+    Both searches run the same cross-entropy method (cutauleaping_b200.fitsearch)
+    until their best true fitness is within 2% of the fitness of the true
+    parameters (the attainable floor at this replicate count), or a generation
+    cap.  The surrogate search pays for its training data and training inside
+    its wall time.  fits/s = 1 / wall seconds to reach that level; when plain
+    search does not reach it within the cap, its time is a lower bound."""
     import torch
     from cutauleaping_b200 import fitsearch as fs
     full = a.full
     n_rep = 512 if full else 64
     n_traj = (1 << 20) if full else (1 << 16)
     screen = 1_000_000 if full else 100_000
-    gens, pop = (8, 10_000) if full else (6, 1000)
+    pop = 10_000 if full else 1000
+    max_gen = 12 if full else 30
     p = fs.make_problem(n_rep=n_rep, samples=50, t_end=5.0)
+    truth = float(fs.true_fitness(p, p.theta_true[None, :], seed=4242)[0])
+    level = truth * 1.02
+
+    def run_until(mode, offset, **kw):
+        hist = fs.cem(p, mode=mode, generations=max_gen, pop=pop, seed=1, stop_at=level, **kw)
+        reached = hist[-1][2] <= level
+        return offset + hist[-1][0], hist[-1][1], reached, hist
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    plain = fs.cem(p, mode="plain", generations=gens, pop=pop, seed=1)
-    t_plain = time.perf_counter() - t0
+    tp, sp, plain_ok, ph = run_until("plain", 0.0)
     t0 = time.perf_counter()
     theta, traj = fs.training_data(p, n_traj)
     torch.cuda.synchronize()
@@ -205,32 +213,23 @@ def bench_config5(a):
     net, sc = fs.train_surrogate(p, theta, traj, epochs=2, batch=16384)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0 - t_data
-    surr = fs.cem(p, mode="surrogate", generations=gens, pop=pop, screen=screen, keep_frac=0.01, net=net,
-                  sc=sc, seed=1)
-    pre = t_data + t_train
-    f_star = max(plain[-1][2], surr[-1][2]) * 1.02
-
-    def reach(hist, offset):
-        for wall, sims, f, _ in hist:
-            if f <= f_star:
-                return offset + wall, sims
-        return offset + hist[-1][0], hist[-1][1]
-    tp, sp = reach(plain, 0.0)
-    ts, ss = reach(surr, pre)
-    truth = fs.true_fitness(p, p.theta_true[None, :], seed=4242)[0]
+    ts, ss, surr_ok, sh = run_until("surrogate", t_data + t_train, screen=screen, keep_frac=0.01, net=net, sc=sc)
     print(json.dumps({
         "metric": METRIC, "config": {"workload": "surrogate-screened parameter estimation: 32x64 network "
                                                  "(generator seed 1), 8 unknown rate constants, target = mean "
                                                  f"of {n_rep} simulations at 50 instants", "full_size": full,
                                      "n_rep": n_rep, "training_trajectories": n_traj, "screened_per_gen": screen,
-                                     "resimulated_per_gen": pop, "generations": gens},
+                                     "resimulated_per_gen": pop, "max_generations": max_gen},
         "value": 1.0 / ts, "unit": "fits/s (surrogate-screened)", "plain_fits_per_s": 1.0 / tp,
-        "speedup_vs_plain": tp / ts, "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
-        "final_fitness": {"plain": plain[-1][2], "surrogate": surr[-1][2], "true_parameters": float(truth),
-                          "common_level": f_star},
+        "speedup_vs_plain": tp / ts, "speedup_is_lower_bound": not plain_ok, "surrogate_reached": surr_ok,
+        "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+        "fitness": {"true_parameters": truth, "level": level, "plain_best": ph[-1][2], "surrogate_best": sh[-1][2]},
         "time_s": {"plain_to_level": tp, "surrogate_to_level": ts, "surrogate_data": t_data,
-                   "surrogate_training": t_train, "plain_total": t_plain},
+                   "surrogate_training": t_train},
+        "generations": {"plain": len(ph), "surrogate": len(sh)},
         "simulations_to_level": {"plain": sp, "surrogate": ss},
+        "curves": {"plain": [[round(h[0], 3), h[2]] for h in ph],
+                   "surrogate": [[round(h[0] + t_data + t_train, 3), h[2]] for h in sh]},
     }), flush=True)
 
 

@@ -1239,6 +1239,75 @@ static int heuristic_group(const HostTables& t) {
 
 // Launch shape for (model, cfg, n): group size, threads, slots and grid.
 // Small batches use smaller blocks so that every SM gets work.
+// Device attributes and kernel occupancy, cached: querying them costs far
+// more than a small sweep launch.
+struct DevAttr {
+    int sm_count = 0, smem_optin = 0;
+};
+static std::mutex g_attr_mu;
+static DevAttr g_attr[16];
+
+static ctl_status device_attr(int dev, DevAttr& out) {
+    if (dev < 0 || dev >= 16) return CTL_ERR_ARG;
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    if (!g_attr[dev].sm_count) {
+        DevAttr a;
+        CTL_CUDA(cudaDeviceGetAttribute(&a.sm_count, cudaDevAttrMultiProcessorCount, dev));
+        CTL_CUDA(cudaDeviceGetAttribute(&a.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        g_attr[dev] = a;
+    }
+    out = g_attr[dev];
+    return CTL_OK;
+}
+
+struct OccKey {
+    int dev, G, threads;
+    size_t smem;
+    int bps, regs;
+};
+static std::vector<OccKey> g_occ;
+
+static ctl_status occupancy(int dev, int G, int threads, size_t smem, int& bps, int& regs) {
+    DevAttr da;
+    if (device_attr(dev, da) != CTL_OK) return CTL_ERR_CUDA;
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    for (const auto& o : g_occ)
+        if (o.dev == dev && o.G == G && o.threads == threads && o.smem == smem) {
+            bps = o.bps;
+            regs = o.regs;
+            return CTL_OK;
+        }
+    const void* k = kernel_for(G);
+    // The attribute is a per-kernel ceiling: set it once to the device's
+    // opt-in maximum so that every shape (cached or new) can launch.
+    bool ceiling = false;
+    for (const auto& o : g_occ) ceiling = ceiling || (o.dev == dev && o.G == G);
+    if (!ceiling) {
+        CTL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, g_attr[dev].smem_optin));
+    }
+    CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, smem));
+    cudaFuncAttributes fa;
+    CTL_CUDA(cudaFuncGetAttributes(&fa, k));
+    regs = fa.numRegs;
+    g_occ.push_back({dev, G, threads, smem, bps, regs});
+    return CTL_OK;
+}
+
+// Host-buffer runs stage through stream-ordered allocations; keep the
+// device's default pool from returning that memory to the driver at every
+// synchronisation, so that repeated calls reuse it.
+static void keep_pool_memory(int dev) {
+    static bool done[16];
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    if (dev < 0 || dev >= 16 || done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done[dev] = true;
+}
+
 static uint32_t n_bucket(uint32_t n) {
     uint32_t b = 0;
     while ((1u << b) < n && b < 31) b++;
@@ -1284,12 +1353,12 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
         return CTL_ERR_ARG;
     }
     int dev_id = cfg->device;
-    cudaDeviceProp prop;
-    CTL_CUDA(cudaGetDeviceProperties(&prop, dev_id));
-    const size_t smem_max = prop.sharedMemPerBlockOptin;
+    DevAttr da;
+    if (device_attr(dev_id, da) != CTL_OK) return CTL_ERR_CUDA;
+    const size_t smem_max = (size_t)da.smem_optin;
     const bool uni = cfg->uniform_rates != 0;
     if (cfg->threads <= 0) {
-        while (threads > 32 && (uint64_t)n * G < (uint64_t)threads * prop.multiProcessorCount) threads -= 32;
+        while (threads > 32 && (uint64_t)n * G < (uint64_t)threads * da.sm_count) threads -= 32;
     }
     for (;;) {
         int NS = threads / G;
@@ -1308,21 +1377,17 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     }
     pl.G = G;
     pl.threads = threads;
-    const void* k = kernel_for(G);
-    CTL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));
-    int bps = 0;
-    CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, pl.smem));
+    int bps = 0, regs = 0;
+    if (occupancy(dev_id, G, threads, pl.smem, bps, regs) != CTL_OK) return CTL_ERR_CUDA;
     if (bps < 1) {
         set_error("sweep kernel cannot be resident with this shape");
         return CTL_ERR_SHAPE;
     }
-    cudaFuncAttributes fa;
-    CTL_CUDA(cudaFuncGetAttributes(&fa, k));
-    pl.regs = fa.numRegs;
+    pl.regs = regs;
     pl.blocks_per_sm = bps;
-    pl.sm_count = prop.multiProcessorCount;
+    pl.sm_count = da.sm_count;
     uint64_t need = (n + (uint64_t)pl.NS - 1) / pl.NS;
-    uint64_t cap = (uint64_t)bps * prop.multiProcessorCount;
+    uint64_t cap = (uint64_t)bps * da.sm_count;
     pl.blocks = (int)std::max<uint64_t>(1, std::min(need, cap));
     return CTL_OK;
 }
@@ -1469,6 +1534,7 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
     if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;
     const size_t bx = (size_t)n * t.S * 4, bc = (size_t)n * t.R * 4;
     const size_t bo = (size_t)n * t.ns * t.s_out * 4, bi = (size_t)n * sizeof(ctl_sim_info);
+    keep_pool_memory(cfg->device);
     cudaStream_t s;
     CTL_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     void *dx = nullptr, *dc = nullptr, *dout = nullptr, *dinf = nullptr;

@@ -202,7 +202,7 @@ def predicted_fitness(p: FitProblem, net, sc, theta_log, *, chunk=65536):
 # ---------------------------------------------------------------------------
 
 def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_frac=0.01, net=None,
-        sc=None, seed=0, sim_seed=1000, time_limit=None):
+        sc=None, seed=0, sim_seed=1000, time_limit=None, stop_at=None):
     """Cross-entropy search in log-parameter space.  mode 'plain' simulates
     every candidate; mode 'surrogate' screens `screen` candidates per
     generation and simulates the best keep_frac of them.  Returns a list of
@@ -233,5 +233,7 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
         sd = np.maximum(el.std(0), 0.02 * (p.log_hi - p.log_lo))
         hist.append((time.perf_counter() - t0, sims, best_f, best_t))
         if time_limit is not None and time.perf_counter() - t0 > time_limit:
+            break
+        if stop_at is not None and best_f <= stop_at:
             break
     return hist
