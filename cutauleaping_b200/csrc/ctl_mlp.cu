@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <algorithm>
 #include <string>
 
 #include "ctl_internal.h"
@@ -326,6 +327,316 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
     }
 }
 
+
+// ---- fused screening: input build -> 5 layers -> fitness, one kernel --------------
+//
+// Screening scores candidates by the surrogate's ensemble mean: rows are
+// (candidate, sample instant) pairs, row = cand * ns + ti.  One CTA owns a
+// 128-row tile at a time (persistent over tiles) and keeps the tile's
+// activations in shared memory for all five layers, so HBM sees only the
+// candidates' parameters and one fitness word per candidate:
+//   * warps 0-3 (epilogue): build the layer-0 input rows, then per layer read
+//     the TMEM accumulator (warp w owns rows 32w..32w+31), add bias, SiLU,
+//     round to BF16 and write the next layer's A operand in place; after the
+//     last layer they accumulate sum_s |target - mean| / target per row and
+//     reduce rows to candidates in shared memory;
+//   * warp 4 (producer): streams the packed weights, 32 K-columns per stage,
+//     with bulk asynchronous copies completing on per-stage mbarriers;
+//   * warp 5 (MMA): one thread issues tcgen05.mma (M = 128, N = layer width,
+//     K = 16) from the activation tile and the weight stage into TMEM.
+// Two CTAs share an SM, so one CTA's epilogue overlaps the other's MMAs.
+constexpr int SC_BK = 32, SC_STAGES = 3, SC_THREADS = 192, SC_HID = 256, SC_LAYERS = 5;
+constexpr int SC_A_BYTES = 128 * SC_HID * 2;
+constexpr int SC_STAGE_BYTES = SC_HID * SC_BK * 2;
+
+struct Screen {
+    const float* theta;   // [n_cand][n_par]
+    int n_par;
+    uint32_t n_cand, ns, n_rows, n_tiles;
+    const float* tvec;    // [ns]
+    float t_end;
+    const float* log_lo;  // [n_par]
+    const float* log_hi;
+    const float* y_mean;  // [S]
+    const float* y_std;
+    int S, out_w;
+    const float* target;  // [ns][S]
+    const uint8_t* wpack; // packed BF16 weights (ctl_mlp_pack)
+    const float* bias;    // [4*256 + out_w]
+    double* fit;          // [n_cand] sums, zeroed by the caller
+    unsigned* err;
+};
+
+__device__ __forceinline__ int sc_k(int l) { return l == 0 ? 64 : SC_HID; }
+__device__ __forceinline__ int sc_n(const Screen& p, int l) { return l == SC_LAYERS - 1 ? p.out_w : SC_HID; }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+// Named barrier over the 128 epilogue threads (warps 0-3), and the same
+// barrier as a vote: true when every epilogue thread passes true.
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+__device__ __forceinline__ bool epi_all(bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred a, b;\n\t"
+        "setp.ne.u32 a, %1, 0;\n\t"
+        "bar.red.and.pred b, 1, 128, a;\n\t"
+        "selp.u32 %0, 1, 0, b;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v)
+        : "memory");
+    return r != 0;
+}
+
+// Byte offset of (row, k) in a K-major no-swizzle tile with `rows` rows.
+__device__ __forceinline__ uint32_t canon(int row, int k, int rows) {
+    return (uint32_t)(((k >> 3) * (rows >> 3) + (row >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
+    const __nv_bfloat16 x = __float2bfloat16(a), y = __float2bfloat16(b);
+    return (uint32_t)__bfloat16_as_ushort(x) | ((uint32_t)__bfloat16_as_ushort(y) << 16);
+}
+
+// Layer-0 input of row r of the tile: scaled log parameters in [-1, 1],
+// scaled time, zeros (the same FP32 operations as surrogate.make_inputs).
+__device__ void sc_build_input(const Screen& p, uint8_t* A, int r, uint32_t row) {
+    float x[64];
+#pragma unroll
+    for (int j = 0; j < 64; j++) x[j] = 0.0f;
+    if (row < p.n_rows) {
+        const uint32_t cand = row / p.ns, ti = row % p.ns;
+        for (int j = 0; j < p.n_par; j++) {
+            const float lo = p.log_lo[j], hi = p.log_hi[j];
+            const float v = (2.0f * (p.theta[(size_t)cand * p.n_par + j] - lo)) / (hi - lo) - 1.0f;
+#pragma unroll
+            for (int q = 0; q < 64; q++)
+                if (q == j) x[q] = v;
+        }
+        const float tv = (2.0f * p.tvec[ti]) / p.t_end - 1.0f;
+#pragma unroll
+        for (int q = 0; q < 64; q++)
+            if (q == p.n_par) x[q] = tv;
+    }
+#pragma unroll
+    for (int kb = 0; kb < 8; kb++) {
+        uint4 v;
+        v.x = pack_bf2(x[kb * 8 + 0], x[kb * 8 + 1]);
+        v.y = pack_bf2(x[kb * 8 + 2], x[kb * 8 + 3]);
+        v.z = pack_bf2(x[kb * 8 + 4], x[kb * 8 + 5]);
+        v.w = pack_bf2(x[kb * 8 + 6], x[kb * 8 + 7]);
+        *reinterpret_cast<uint4*>(A + canon(r, kb * 8, 128)) = v;
+    }
+}
+
+__global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t full[SC_STAGES], empty[SC_STAGES], acc_full, a_ready, drain;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag;
+    __shared__ float s_acc[132];
+    uint8_t* A = smem;
+    uint8_t* stage = smem + SC_A_BYTES;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < SC_STAGES; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(&acc_full, 1);
+        mbar_init(&a_ready, 128);
+        mbar_init(&drain, 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = threadIdx.x; i < 132; i += SC_THREADS) s_acc[i] = 0.0f;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_slot)), "r"(SC_HID));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 4) {
+        // ---- producer: the weight stream, repeated for every tile ----
+        if (lane == 0) {
+            uint32_t idx = 0;
+            uint32_t issued[SC_STAGES] = {0u, 0u, 0u};  // copies issued per slot
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x) {
+                size_t off = 0;
+                for (int l = 0; l < SC_LAYERS && ok; l++) {
+                    const uint32_t bytes = (uint32_t)(sc_n(p, l) * SC_BK * 2);
+                    for (int ks = 0; ks < sc_k(l) / SC_BK; ks++, idx++) {
+                        const uint32_t slot = idx % SC_STAGES, round = idx / SC_STAGES;
+                        if (round > 0 && !mbar_wait(&empty[slot], (round - 1) & 1u, p.err)) { ok = false; break; }
+                        if (*(volatile int*)&abort_flag) { ok = false; break; }
+                        mbar_expect_tx(&full[slot], bytes);
+                        bulk_g2s(stage + slot * SC_STAGE_BYTES, p.wpack + off, bytes, &full[slot]);
+                        issued[slot]++;
+                        off += bytes;
+                    }
+                }
+            }
+            if (!ok) {
+                atomicExch(&abort_flag, 1);
+                // let the copies in flight land before the CTA exits
+                for (int sl = 0; sl < SC_STAGES; sl++)
+                    if (issued[sl]) mbar_wait(&full[sl], (issued[sl] - 1) & 1u, nullptr);
+            }
+        }
+    } else if (warp == 5) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            uint32_t idx = 0, nready = 0;
+            bool ok = true;
+            const uint32_t a0 = smem_u32(A), s0 = smem_u32(stage);
+            for (uint32_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x) {
+                for (int l = 0; l < SC_LAYERS && ok; l++) {
+                    if (!mbar_wait(&a_ready, nready & 1u, p.err) || *(volatile int*)&abort_flag) { ok = false; break; }
+                    nready++;
+                    tc_fence_after();
+                    const int N = sc_n(p, l);
+                    const uint32_t idesc = make_idesc(128, N);
+                    for (int ks = 0; ks < sc_k(l) / SC_BK; ks++, idx++) {
+                        const uint32_t slot = idx % SC_STAGES, round = idx / SC_STAGES;
+                        if (!mbar_wait(&full[slot], round & 1u, p.err)) { ok = false; break; }
+                        tc_fence_after();
+#pragma unroll
+                        for (int kk = 0; kk < SC_BK / 16; kk++) {
+                            const int k0 = ks * SC_BK + kk * 16;  // K offset in the activation tile
+                            const uint64_t da = make_desc(a0 + (uint32_t)(k0 / 8) * 16u * 128u, 16u * 128u, 128u);
+                            const uint64_t db = make_desc(s0 + slot * SC_STAGE_BYTES + (uint32_t)(kk * 2 * (N / 8) * 128),
+                                                          (uint32_t)((N / 8) * 128), 128u);
+                            mma_bf16(tmem, da, db, idesc, (ks > 0 || kk > 0) ? 1u : 0u);
+                        }
+                        mma_commit(&empty[slot]);
+                    }
+                    if (ok) mma_commit(&acc_full);
+                }
+            }
+            if (!ok) atomicExch(&abort_flag, 1);
+            mma_commit(&drain);  // every MMA this thread issued has completed once drain flips
+            mbar_wait(&drain, 0u, nullptr);
+        }
+    } else {
+        // ---- epilogue warps 0-3: thread r owns row r of the tile ----
+        const int r = threadIdx.x;
+        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+        uint32_t nacc = 0;
+        bool ok = true;
+        for (uint32_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x) {
+            const uint32_t row = t * 128u + (uint32_t)r;
+            sc_build_input(p, A, r, row);
+            fence_async_smem();
+            tc_fence_before();
+            mbar_arrive(&a_ready);
+            for (int l = 0; l < SC_LAYERS; l++) {
+                bool got = mbar_wait(&acc_full, nacc & 1u, p.err);
+                got = epi_all(got && !*(volatile int*)&abort_flag);  // uniform: the epilogue holds named barriers
+                nacc++;
+                if (!got) { ok = false; break; }
+                tc_fence_after();
+                if (l < SC_LAYERS - 1) {
+                    const float* b = p.bias + l * SC_HID;
+                    for (int c = 0; c < SC_HID; c += 16) {
+                        float v[16];
+                        tmem_ld16(tmem + lane_base + (uint32_t)c, v);
+                        uint32_t h[8];
+#pragma unroll
+                        for (int j = 0; j < 8; j++) {
+                            const float z0 = v[2 * j] + b[c + 2 * j], z1 = v[2 * j + 1] + b[c + 2 * j + 1];
+                            h[j] = pack_bf2(silu(z0), silu(z1));
+                        }
+                        *reinterpret_cast<uint4*>(A + canon(r, c, 128)) = make_uint4(h[0], h[1], h[2], h[3]);
+                        *reinterpret_cast<uint4*>(A + canon(r, c + 8, 128)) = make_uint4(h[4], h[5], h[6], h[7]);
+                    }
+                    fence_async_smem();
+                    tc_fence_before();
+                    mbar_arrive(&a_ready);
+                } else {
+                    // fitness terms of this row: sum_s |target - mean| (/ target when nonzero)
+                    const float* b = p.bias + (SC_LAYERS - 1) * SC_HID;
+                    float acc = 0.0f;
+                    const uint32_t ti = row % p.ns;
+                    for (int c = 0; c < p.S; c += 16) {
+                        float v[16];
+                        tmem_ld16(tmem + lane_base + (uint32_t)c, v);
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            const int s_ = c + j;
+                            if (s_ < p.S && row < p.n_rows) {
+                                const float mean = (v[j] + b[s_]) * p.y_std[s_] + p.y_mean[s_];
+                                const float tg = p.target[(size_t)ti * p.S + s_];
+                                float d = fabsf(tg - mean);
+                                if (tg != 0.0f) d = d / tg;
+                                acc += d;
+                            }
+                        }
+                    }
+                    tc_fence_before();
+                    const uint32_t cand0 = (t * 128u) / p.ns;
+                    if (row < p.n_rows) atomicAdd(&s_acc[row / p.ns - cand0], acc);
+                    epi_sync();
+                    const uint32_t last = (min(t * 128u + 127u, p.n_rows - 1u)) / p.ns;
+                    if ((uint32_t)r <= last - cand0 && t * 128u < p.n_rows) {
+                        atomicAdd(&p.fit[cand0 + r], (double)s_acc[r]);
+                        s_acc[r] = 0.0f;
+                    }
+                    epi_sync();
+                }
+            }
+        }
+        if (!ok) atomicExch(&abort_flag, 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(SC_HID));
+}
+
+// Packs a BF16 weight matrix W [N][K] (K contiguous, row stride ldw) into
+// K-stages of 32 columns, each stage N x 32 in the canonical K-major layout,
+// stages consecutive: the screening kernel copies one stage per bulk copy.
+__global__ void pack_kernel(const __nv_bfloat16* __restrict__ W, int N, int K, int ldw,
+                            __nv_bfloat16* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N * K) return;
+    const int n = i / K, k = i % K;
+    const int ks = k / SC_BK, kin = k % SC_BK;
+    const size_t o = (size_t)ks * N * SC_BK + canon(n, kin, N) / 2;
+    out[o] = W[(size_t)n * ldw + k];
+}
+
+__global__ void scale_kernel(double* f, uint32_t n, double s) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) f[i] *= s;
+}
+
 }  // namespace mlp
 }  // namespace ctl
 
@@ -404,4 +715,78 @@ extern "C" ctl_status ctl_mlp_adam(float* w, const float* g, float* m1, float* m
         w, g, m1, m2, n, rows, cols, lr, beta1, beta2, eps, c1, c2, wd, static_cast<__nv_bfloat16*>(wb),
         static_cast<__nv_bfloat16*>(wbT));
     return mlp_cuda(cudaGetLastError(), "adam_kernel launch");
+}
+
+extern "C" size_t ctl_mlp_pack_bytes(int32_t out_w) {
+    return (size_t)2 * (256 * 64 + 3 * 256 * 256 + (size_t)out_w * 256);
+}
+
+extern "C" ctl_status ctl_mlp_pack(const void* const* W, const int32_t* ldw, int32_t out_w, void* wpack,
+                                   void* stream) {
+    if (!W || !ldw || !wpack || out_w <= 0 || out_w % 16 || out_w > 256) return CTL_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(wpack) % 16) {
+        set_error("ctl_mlp_pack: output must be 16-byte aligned");
+        return CTL_ERR_ARG;
+    }
+    auto* out = static_cast<__nv_bfloat16*>(wpack);
+    size_t off = 0;
+    for (int l = 0; l < mlp::SC_LAYERS; l++) {
+        const int N = l == mlp::SC_LAYERS - 1 ? out_w : mlp::SC_HID, K = l == 0 ? 64 : mlp::SC_HID;
+        if (!W[l] || ldw[l] < K) return CTL_ERR_ARG;
+        mlp::pack_kernel<<<(N * K + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+            static_cast<const __nv_bfloat16*>(W[l]), N, K, ldw[l], out + off);
+        ctl_status st = mlp_cuda(cudaGetLastError(), "pack_kernel launch");
+        if (st != CTL_OK) return st;
+        off += (size_t)N * K;
+    }
+    return CTL_OK;
+}
+
+extern "C" ctl_status ctl_mlp_screen(const ctl_screen_desc* d, void* stream) {
+    if (!d || !d->theta || !d->tvec || !d->log_lo || !d->log_hi || !d->y_mean || !d->y_std || !d->target ||
+        !d->wpack || !d->bias || !d->fitness)
+        return CTL_ERR_ARG;
+    if (d->n_par < 1 || d->n_par > 63 || d->ns == 0 || d->S < 1 || 2 * d->S > d->out_w || d->out_w % 16 ||
+        d->out_w > 256 || !(d->t_end > 0.0f)) {
+        set_error("ctl_mlp_screen: need 1 <= n_par <= 63, ns >= 1, 2*S <= out_w <= 256, out_w % 16 == 0, t_end > 0");
+        return CTL_ERR_SHAPE;
+    }
+    if (reinterpret_cast<uintptr_t>(d->wpack) % 16) {
+        set_error("ctl_mlp_screen: packed weights must be 16-byte aligned");
+        return CTL_ERR_ARG;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    ctl_status st = mlp_cuda(cudaMemsetAsync(d->fitness, 0, sizeof(double) * d->n_cand, s), "memset fitness");
+    if (st != CTL_OK || d->n_cand == 0) return st;
+    const uint64_t rows = (uint64_t)d->n_cand * d->ns;
+    if (rows > 0xffffff00ull) {
+        set_error("ctl_mlp_screen: n_cand * ns must fit in 32 bits");
+        return CTL_ERR_SHAPE;
+    }
+    mlp::Screen p;
+    p.theta = d->theta; p.n_par = d->n_par; p.n_cand = d->n_cand; p.ns = d->ns;
+    p.n_rows = (uint32_t)rows; p.n_tiles = (uint32_t)((rows + 127) / 128);
+    p.tvec = d->tvec; p.t_end = d->t_end; p.log_lo = d->log_lo; p.log_hi = d->log_hi;
+    p.y_mean = d->y_mean; p.y_std = d->y_std; p.S = d->S; p.out_w = d->out_w; p.target = d->target;
+    p.wpack = static_cast<const uint8_t*>(d->wpack); p.bias = d->bias; p.fit = d->fitness; p.err = d->err;
+    const size_t smem = (size_t)mlp::SC_A_BYTES + (size_t)mlp::SC_STAGES * mlp::SC_STAGE_BYTES;
+    static int sms[16];
+    int dev = 0;
+    if ((st = mlp_cuda(cudaGetDevice(&dev), "cudaGetDevice")) != CTL_OK) return st;
+    if (dev < 0 || dev >= 16) return CTL_ERR_ARG;
+    if (!sms[dev]) {
+        if ((st = mlp_cuda(cudaFuncSetAttribute(mlp::screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)smem), "cudaFuncSetAttribute(screen)")) != CTL_OK)
+            return st;
+        int n = 0;
+        if ((st = mlp_cuda(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev), "sm count")) != CTL_OK)
+            return st;
+        sms[dev] = n;
+    }
+    const uint32_t grid = std::min<uint32_t>(p.n_tiles, 2u * (uint32_t)sms[dev]);
+    mlp::screen_kernel<<<grid, mlp::SC_THREADS, smem, s>>>(p);
+    if ((st = mlp_cuda(cudaGetLastError(), "screen_kernel launch")) != CTL_OK) return st;
+    mlp::scale_kernel<<<(d->n_cand + 255) / 256, 256, 0, s>>>(d->fitness, d->n_cand,
+                                                              1.0 / ((double)d->ns * (double)d->S));
+    return mlp_cuda(cudaGetLastError(), "scale_kernel launch");
 }

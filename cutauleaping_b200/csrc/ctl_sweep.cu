@@ -1260,36 +1260,59 @@ static ctl_status device_attr(int dev, DevAttr& out) {
     return CTL_OK;
 }
 
+// Per (device, G): the kernel's registers and the largest dynamic shared
+// memory a launch may ask for (the opt-in maximum less the kernel's static
+// shared memory).  The first query raises the kernel's dynamic-memory
+// ceiling to that limit once, so every shape (cached or new) can launch.
+struct KernAttr {
+    int dev, G, regs;
+    size_t dyn_max;
+};
+static std::vector<KernAttr> g_kattr;
+
+static ctl_status kernel_attr(int dev, int G, KernAttr& out) {
+    DevAttr da;
+    if (device_attr(dev, da) != CTL_OK) return CTL_ERR_CUDA;
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    for (const auto& a : g_kattr)
+        if (a.dev == dev && a.G == G) {
+            out = a;
+            return CTL_OK;
+        }
+    const void* k = kernel_for(G);
+    cudaFuncAttributes fa;
+    CTL_CUDA(cudaFuncGetAttributes(&fa, k));
+    if ((size_t)da.smem_optin <= fa.sharedSizeBytes) {
+        set_error("sweep kernel's static shared memory exceeds the device limit");
+        return CTL_ERR_SHAPE;
+    }
+    KernAttr a{dev, G, fa.numRegs, (size_t)da.smem_optin - fa.sharedSizeBytes};
+    CTL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.dyn_max));
+    g_kattr.push_back(a);
+    out = a;
+    return CTL_OK;
+}
+
 struct OccKey {
     int dev, G, threads;
     size_t smem;
-    int bps, regs;
+    int bps;
 };
 static std::vector<OccKey> g_occ;
 
 static ctl_status occupancy(int dev, int G, int threads, size_t smem, int& bps, int& regs) {
-    DevAttr da;
-    if (device_attr(dev, da) != CTL_OK) return CTL_ERR_CUDA;
+    KernAttr ka;
+    ctl_status st = kernel_attr(dev, G, ka);
+    if (st != CTL_OK) return st;
+    regs = ka.regs;
     std::lock_guard<std::mutex> lk(g_attr_mu);
     for (const auto& o : g_occ)
         if (o.dev == dev && o.G == G && o.threads == threads && o.smem == smem) {
             bps = o.bps;
-            regs = o.regs;
             return CTL_OK;
         }
-    const void* k = kernel_for(G);
-    // The attribute is a per-kernel ceiling: set it once to the device's
-    // opt-in maximum so that every shape (cached or new) can launch.
-    bool ceiling = false;
-    for (const auto& o : g_occ) ceiling = ceiling || (o.dev == dev && o.G == G);
-    if (!ceiling) {
-        CTL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, g_attr[dev].smem_optin));
-    }
-    CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, smem));
-    cudaFuncAttributes fa;
-    CTL_CUDA(cudaFuncGetAttributes(&fa, k));
-    regs = fa.numRegs;
-    g_occ.push_back({dev, G, threads, smem, bps, regs});
+    CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel_for(G), threads, smem));
+    g_occ.push_back({dev, G, threads, smem, bps});
     return CTL_OK;
 }
 
@@ -1355,7 +1378,9 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     int dev_id = cfg->device;
     DevAttr da;
     if (device_attr(dev_id, da) != CTL_OK) return CTL_ERR_CUDA;
-    const size_t smem_max = (size_t)da.smem_optin;
+    KernAttr ka;
+    if (ctl_status st = kernel_attr(dev_id, G, ka); st != CTL_OK) return st;
+    const size_t smem_max = ka.dyn_max;
     const bool uni = cfg->uniform_rates != 0;
     if (cfg->threads <= 0) {
         while (threads > 32 && (uint64_t)n * G < (uint64_t)threads * da.sm_count) threads -= 32;
@@ -1378,7 +1403,7 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     pl.G = G;
     pl.threads = threads;
     int bps = 0, regs = 0;
-    if (occupancy(dev_id, G, threads, pl.smem, bps, regs) != CTL_OK) return CTL_ERR_CUDA;
+    if (ctl_status st = occupancy(dev_id, G, threads, pl.smem, bps, regs); st != CTL_OK) return st;
     if (bps < 1) {
         set_error("sweep kernel cannot be resident with this shape");
         return CTL_ERR_SHAPE;

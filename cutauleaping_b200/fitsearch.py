@@ -169,8 +169,17 @@ def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-
     return net, sc
 
 
-def predicted_fitness(p: FitProblem, net, sc, theta_log, *, chunk=65536):
-    """Reference fitness computed from the surrogate's ensemble mean."""
+def predicted_fitness(p: FitProblem, net, sc, theta_log):
+    """Reference fitness computed from the surrogate's ensemble mean, in the
+    fused screening kernel (ctl_mlp_screen)."""
+    import torch
+    theta = torch.as_tensor(np.asarray(theta_log), dtype=torch.float32, device="cuda")
+    return sg.screen(net, theta, p.tvec, p.target.astype(np.float32), sc).cpu().numpy()
+
+
+def predicted_fitness_layers(p: FitProblem, net, sc, theta_log, *, chunk=65536):
+    """The same fitness through the layer-by-layer path (one tcgen05 GEMM
+    per layer, fitness in PyTorch): the cross-check of the fused kernel."""
     import torch
     theta_log = torch.as_tensor(np.asarray(theta_log), dtype=torch.float32, device="cuda")
     n = theta_log.shape[0]
@@ -202,15 +211,23 @@ def predicted_fitness(p: FitProblem, net, sc, theta_log, *, chunk=65536):
 # ---------------------------------------------------------------------------
 
 def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_frac=0.01, net=None,
-        sc=None, seed=0, sim_seed=1000, time_limit=None, stop_at=None):
-    """Cross-entropy search in log-parameter space.  mode 'plain' simulates
-    every candidate; mode 'surrogate' screens `screen` candidates per
-    generation and simulates the best keep_frac of them.  Returns a list of
-    (wall seconds, simulations so far, best true fitness, best theta)."""
+        sc=None, seed=0, sim_seed=1000, time_limit=None, stop_at=None, inner=1):
+    """Cross-entropy search in log-parameter space.
+
+    mode 'plain' simulates every one of `pop` candidates per generation.
+    mode 'surrogate' runs, per generation, `inner` surrogate-only CEM
+    iterations from the current proposal (each screens `screen` candidates
+    and refits the proposal to the best `elite` fraction by predicted
+    fitness; the last one keeps its screened set), then re-simulates the best
+    max(pop, keep_frac * screen) screened candidates and refits the proposal
+    to their best by true fitness.  Every candidate whose fitness is reported
+    was simulated.  Returns a list of (wall seconds, simulations so far, best
+    true fitness, best theta), one entry per generation."""
     rng = np.random.default_rng(seed)
     d = len(p.unknown)
     mu = (p.log_lo + p.log_hi) / 2
     sd = (p.log_hi - p.log_lo) / 2
+    floor = 0.02 * (p.log_hi - p.log_lo)
     best_f, best_t = math.inf, None
     hist = []
     sims = 0
@@ -219,9 +236,14 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
         if mode == "plain":
             cand = np.clip(rng.normal(mu, sd, size=(pop, d)), p.log_lo, p.log_hi)
         else:
-            big = np.clip(rng.normal(mu, sd, size=(screen, d)), p.log_lo, p.log_hi)
-            pf = predicted_fitness(p, net, sc, big)
-            cand = big[np.argsort(pf)[: max(pop, int(keep_frac * screen))]]
+            for it in range(inner):
+                big = np.clip(rng.normal(mu, sd, size=(screen, d)), p.log_lo, p.log_hi)
+                order = np.argsort(predicted_fitness(p, net, sc, big))
+                if it < inner - 1:
+                    el = big[order[: max(2, int(elite * keep_frac * screen))]]
+                    mu = el.mean(0)
+                    sd = np.maximum(el.std(0), floor)
+            cand = big[order[: max(pop, int(keep_frac * screen))]]
         f = true_fitness(p, cand, seed=sim_seed + gen, sim_base=0)
         sims += len(cand) * p.n_rep
         order = np.argsort(f)
@@ -230,7 +252,7 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
         ne = max(2, int(elite * len(cand)))
         el = cand[order[:ne]]
         mu = el.mean(0)
-        sd = np.maximum(el.std(0), 0.02 * (p.log_hi - p.log_lo))
+        sd = np.maximum(el.std(0), floor)
         hist.append((time.perf_counter() - t0, sims, best_f, best_t))
         if time_limit is not None and time.perf_counter() - t0 > time_limit:
             break

@@ -9,10 +9,11 @@ with the plain method, which also judges the surrogate's error.
 Network: x = (8 scaled log rate constants, scaled t) -> 256 -> 256 -> 256 ->
 256 -> 2*S (per-species mean and log-variance of the standardised counts),
 SiLU, BF16 weights and activations, FP32 accumulation and master weights,
-Gaussian negative log-likelihood, Adam.  Every matrix product runs in the
-project's own tcgen05 kernel (ctl_mlp_gemm); the loss gradient, bias
-gradients and Adam are the project's own kernels too.  PyTorch only provides
-device memory.
+Gaussian negative log-likelihood, Adam.  Every matrix product of training
+runs in the project's own tcgen05 kernel (ctl_mlp_gemm); the loss gradient,
+bias gradients and Adam are the project's own kernels too.  Screening runs
+the whole network and the fitness in one fused tcgen05 kernel
+(ctl_mlp_screen, `screen`).  PyTorch only provides device memory.
 """
 from __future__ import annotations
 
@@ -38,10 +39,22 @@ class GemmDesc(C.Structure):
                 ("out_bfT", C.c_void_p), ("ldobT", C.c_int32), ("err", C.c_void_p)]
 
 
+class ScreenDesc(C.Structure):
+    _fields_ = [("theta", C.c_void_p), ("n_par", C.c_int32), ("n_cand", C.c_uint32), ("tvec", C.c_void_p),
+                ("ns", C.c_uint32), ("t_end", C.c_float), ("log_lo", C.c_void_p), ("log_hi", C.c_void_p),
+                ("y_mean", C.c_void_p), ("y_std", C.c_void_p), ("S", C.c_int32), ("out_w", C.c_int32),
+                ("target", C.c_void_p), ("wpack", C.c_void_p), ("bias", C.c_void_p), ("fitness", C.c_void_p),
+                ("err", C.c_void_p)]
+
+
 def _bind():
     L = lib()
     if not getattr(L, "_mlp_bound", False):
         P = C.c_void_p
+        L.ctl_mlp_pack_bytes.argtypes = [C.c_int32]
+        L.ctl_mlp_pack_bytes.restype = C.c_size_t
+        L.ctl_mlp_pack.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_int32), C.c_int32, P, P]
+        L.ctl_mlp_screen.argtypes = [C.POINTER(ScreenDesc), P]
         L.ctl_mlp_gemm.argtypes = [C.POINTER(GemmDesc), P]
         L.ctl_mlp_nll_grad.argtypes = [P, C.c_int32, P, C.c_int32, C.c_int32, P, C.c_int32, P, C.c_int32, P, P]
         L.ctl_mlp_colsum.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, P, P]
@@ -213,9 +226,47 @@ class MLP:
             if st != OK:
                 raise CtlError(st, "ctl_mlp_adam")
 
+    def packed(self):
+        """Weights in the screening kernel's streaming layout and the
+        concatenated biases; rebuilt after every Adam step."""
+        torch = self.torch
+        if getattr(self, "_packed_at", None) != self.step_count:
+            L = _bind()
+            wp = torch.empty(L.ctl_mlp_pack_bytes(self.out_w) // 2, dtype=torch.bfloat16, device="cuda")
+            ptrs = (C.c_void_p * 5)(*[w.data_ptr() for w in self.Wb])
+            lds = (C.c_int32 * 5)(*[w.stride(0) for w in self.Wb])
+            st = L.ctl_mlp_pack(ptrs, lds, self.out_w, _ptr(wp), _stream())
+            if st != OK:
+                raise CtlError(st, "ctl_mlp_pack")
+            self._wpack = wp
+            self._bias = torch.cat(self.b).contiguous()
+            self._packed_at = self.step_count
+        return self._wpack, self._bias
+
     def check_error_flag(self):
         if int(self.err.item()) != 0:
             raise RuntimeError("tcgen05 GEMM reported a bounded-wait timeout")
 
     def state_numpy(self):
         return ([w.cpu().numpy() for w in self.W], [b.cpu().numpy() for b in self.b])
+
+
+def screen(net: MLP, theta_log, tvec, target, sc: Scaling):
+    """Fitness of each candidate from the surrogate's ensemble mean, in one
+    fused kernel (ctl_mlp_screen): theta_log [n][n_par] FP32 device tensor,
+    tvec [ns], target [ns][S]; returns a FP64 device tensor [n]."""
+    torch = net.torch
+    L = _bind()
+    dev = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.float32, device="cuda").contiguous()
+    theta = theta_log.to(torch.float32).contiguous()
+    n, n_par = theta.shape
+    tv, tg = dev(tvec), dev(target)
+    lo, hi, ym, ys = dev(sc.log_lo), dev(sc.log_hi), dev(sc.y_mean), dev(sc.y_std)
+    wp, bias = net.packed()
+    fit = torch.empty(n, dtype=torch.float64, device="cuda")
+    d = ScreenDesc(_ptr(theta), n_par, n, _ptr(tv), tv.shape[0], float(sc.t_end), _ptr(lo), _ptr(hi), _ptr(ym),
+                   _ptr(ys), net.S, net.out_w, _ptr(tg), _ptr(wp), _ptr(bias), _ptr(fit), _ptr(net.err))
+    st = L.ctl_mlp_screen(C.byref(d), _stream())
+    if st != OK:
+        raise CtlError(st, "ctl_mlp_screen")
+    return fit

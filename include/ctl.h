@@ -250,6 +250,40 @@ ctl_status ctl_mlp_adam(float* w, const float* g, float* m1, float* m2, int32_t 
                         float lr, float beta1, float beta2, float eps, int32_t step, float weight_decay,
                         void* w_bf16, void* wT_bf16, void* stream);
 
+/* Fused surrogate screening (no reference counterpart: the reference scores
+ * every candidate by full simulation, kernel.cu:365-423).  For each
+ * candidate parameter set, runs the trained MLP at every sample instant and
+ * returns the reference's fitness (calculateFitness,
+ * 2phase_n-tau-leaping.cu:3324-3408) of the predicted ensemble mean against
+ * the target: sum over instants and species of |target - mean| / target
+ * (|target - mean| where the target is 0), divided by ns * S.  One kernel:
+ * activations stay on chip, weights stream from ctl_mlp_pack's buffer. */
+typedef struct {
+    const float* theta;     /* [n_cand][n_par] log rate constants */
+    int32_t n_par;          /* 1..63; network input = n_par scaled parameters + scaled t */
+    uint32_t n_cand;
+    const float* tvec;      /* [ns] sample instants */
+    uint32_t ns;
+    float t_end;            /* time scale of the input */
+    const float* log_lo;    /* [n_par] prior box, maps theta to [-1, 1] */
+    const float* log_hi;
+    const float* y_mean;    /* [S] output de-standardisation: mean = y * y_std + y_mean */
+    const float* y_std;
+    int32_t S;              /* output species (2S <= out_w) */
+    int32_t out_w;          /* output layer width (multiple of 16, <= 256) */
+    const float* target;    /* [ns][S] */
+    const void* wpack;      /* ctl_mlp_pack output (16-byte aligned) */
+    const float* bias;      /* [4*256 + out_w]: the five layers' biases, concatenated */
+    double* fitness;        /* [n_cand] out */
+    unsigned* err;          /* device word, bit 0 raised if a bounded wait timed out */
+} ctl_screen_desc;
+/* Bytes of the packed weights for an output width. */
+size_t ctl_mlp_pack_bytes(int32_t out_w);
+/* Packs BF16 weights W[0] [256][64], W[1..3] [256][256], W[4] [out_w][256]
+ * (row strides ldw[l] elements) for ctl_mlp_screen. */
+ctl_status ctl_mlp_pack(const void* const* W, const int32_t* ldw, int32_t out_w, void* wpack, void* stream);
+ctl_status ctl_mlp_screen(const ctl_screen_desc* d, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

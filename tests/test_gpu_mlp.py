@@ -125,3 +125,80 @@ def test_mlp_training_reduces_nll():
         losses.append(loss.item() / (Bn * S))
     net.check_error_flag()
     assert np.mean(losses[-20:]) < np.mean(losses[:20]) - 1.0, (losses[:3], losses[-3:])
+
+
+def _screen_setup(S, n_cand, ns, seed):
+    """A surrogate with random biases, a candidate set, instants and a
+    target (one zero entry: the absolute-difference branch)."""
+    import math
+    torch = _torch()
+    from cutauleaping_b200 import surrogate as sg
+    net = sg.MLP(S, seed=seed)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    for l in range(len(net.b)):
+        net.b[l].copy_(0.2 * torch.randn(net.b[l].shape, device="cuda", generator=g))
+    rng = np.random.default_rng(seed)
+    lo, hi = np.full(8, math.log(1e-3)), np.zeros(8)
+    sc = sg.Scaling(lo, hi, 5.0, rng.uniform(50, 500, S).astype(np.float32),
+                    rng.uniform(5, 50, S).astype(np.float32))
+    theta = rng.uniform(lo, hi, size=(n_cand, 8)).astype(np.float32)
+    tvec = (5.0 * np.arange(1, ns + 1) / ns).astype(np.float32)
+    target = rng.integers(1, 800, size=(ns, S)).astype(np.float32)
+    target[0, 0] = 0.0
+    return net, sc, theta, tvec, target
+
+
+def _fitness_of_mean(mean, target):
+    d = np.abs(target[None].astype(np.float64) - mean)
+    d = np.where(target[None] != 0, d / np.maximum(target[None], 1), d)
+    return d.sum(axis=(1, 2)) / (target.shape[0] * target.shape[1])
+
+
+@pytest.mark.parametrize("S,n_cand,ns", [(5, 37, 7), (16, 1, 1), (32, 130, 1), (32, 9, 50)])
+def test_screen_matches_cpu_oracle(S, n_cand, ns):
+    """Fused screening (input build, five layers, fitness) against the CPU
+    oracle's forward pass with the same BF16 rounding; tolerance 2e-3
+    relative on each candidate's fitness (BF16 ties may round differently
+    under FP32 vs FP64 accumulation)."""
+    torch = _torch()
+    import oracle.mlp_oracle as mo
+    from cutauleaping_b200 import surrogate as sg
+    net, sc, theta, tvec, target = _screen_setup(S, n_cand, ns, seed=S + n_cand + ns)
+    fit = sg.screen(net, torch.as_tensor(theta, device="cuda"), tvec, target, sc)
+    torch.cuda.synchronize()
+    assert int(net.err.item()) == 0
+    # oracle input rows: the same FP32 operations, then BF16
+    f32 = np.float32
+    th = np.repeat(theta, ns, axis=0)
+    tt = np.tile(tvec, n_cand)
+    X = np.zeros((n_cand * ns, 64), dtype=f32)
+    X[:, :8] = (f32(2.0) * (th - sc.log_lo.astype(f32))) / (sc.log_hi.astype(f32) - sc.log_lo.astype(f32)) - f32(1.0)
+    X[:, 8] = (f32(2.0) * tt) / f32(sc.t_end) - f32(1.0)
+    W = [w.cpu().numpy() for w in net.W]
+    b = [x.cpu().numpy() for x in net.b]
+    y, _, _ = mo.forward(X, W, b)
+    mean = (y[:, :S].astype(np.float64) * sc.y_std + sc.y_mean).reshape(n_cand, ns, S)
+    ref = _fitness_of_mean(mean, target)
+    got = fit.cpu().numpy()
+    assert np.allclose(got, ref, rtol=2e-3, atol=1e-6), np.abs(got / ref - 1).max()
+
+
+def test_screen_matches_layered_path():
+    """Many tiles per CTA: the fused kernel against the layer-by-layer tcgen05
+    GEMM path on the same network (same MMA sequence per layer, so the hidden
+    activations agree; the last step differs only by FP32 vs FP64): 1e-5."""
+    torch = _torch()
+    from cutauleaping_b200 import surrogate as sg
+    S, n_cand, ns = 32, 3001, 50
+    net, sc, theta, tvec, target = _screen_setup(S, n_cand, ns, seed=11)
+    th = torch.as_tensor(theta, device="cuda")
+    fit = sg.screen(net, th, tvec, target, sc).cpu().numpy()
+    rows = n_cand * ns
+    pad = (-rows) % 128
+    X = sg.make_inputs(th.repeat_interleave(ns, 0), torch.as_tensor(tvec, device="cuda").repeat(n_cand), sc, torch)
+    X = torch.cat([X, torch.zeros(pad, X.shape[1], dtype=X.dtype, device="cuda")])
+    y = net.forward(X, keep=False)[:rows, :S].double().cpu().numpy()
+    mean = (y * sc.y_std.astype(np.float64) + sc.y_mean.astype(np.float64)).reshape(n_cand, ns, S)
+    ref = _fitness_of_mean(mean, target)
+    assert int(net.err.item()) == 0
+    assert np.allclose(fit, ref, rtol=1e-5, atol=1e-9), np.abs(fit / ref - 1).max()

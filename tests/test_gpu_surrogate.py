@@ -60,10 +60,12 @@ def test_screening_gains_over_plain_sampling(trained):
     assert f_kept.min() <= f_plain.min()
 
 
-def test_search_runs_and_records_budget(trained):
+@pytest.mark.parametrize("inner", [1, 3])
+def test_search_runs_and_records_budget(trained, inner):
     from cutauleaping_b200 import fitsearch as fs
     p, net, sc, _ = trained
     plain = fs.cem(p, mode="plain", generations=2, pop=64, seed=1)
-    surr = fs.cem(p, mode="surrogate", generations=2, pop=64, screen=6400, keep_frac=0.01, net=net, sc=sc, seed=1)
+    surr = fs.cem(p, mode="surrogate", generations=2, pop=64, screen=6400, keep_frac=0.01, net=net, sc=sc, seed=1,
+                  inner=inner)
     assert surr[-1][1] == plain[-1][1] == 2 * 64 * p.n_rep   # equal simulation budgets
     assert all(h[2] <= g[2] for g, h in zip(surr, surr[1:]))  # best fitness never worsens
