@@ -244,6 +244,8 @@ def main():
     ap.add_argument("--sims", type=int, default=None, help="simulations per GPU (default: config's)")
     ap.add_argument("--group", type=int, default=0, help="lanes per simulation (0 = library choice)")
     ap.add_argument("--threads", type=int, default=0, help="threads per block (0 = library choice)")
+    ap.add_argument("--min-blocks", type=int, default=0,
+                    help="register budget of the sweep kernel: 1, 3 or 4 resident blocks (0 = library choice)")
     ap.add_argument("--autotune", action="store_true", help="measure launch shapes before timing")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -294,7 +296,7 @@ def main():
         model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
         n = net.n
         cfg = ctl.run_cfg(seed=1 + si, sim_base=rank * n, device=local, group=a.group, threads=a.threads,
-                          uniform_rates=int(bool((net.c == net.c[0]).all())))
+                          min_blocks=a.min_blocks, uniform_rates=int(bool((net.c == net.c[0]).all())))
         X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).to(dev)
         c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).to(dev)
         out = torch.empty((n, model.ns, model.s_out), dtype=torch.int32, device=dev)
@@ -429,6 +431,7 @@ def main():
                        "launch": [{"group": pt["li"].group, "threads": pt["li"].threads,
                                    "blocks": pt["li"].blocks, "slots_per_block": pt["li"].slots_per_block,
                                    "smem_bytes": pt["li"].smem_bytes, "regs": pt["li"].regs_per_thread,
+                                   "min_blocks": pt["li"].min_blocks,
                                    "blocks_per_sm": pt["li"].blocks_per_sm} for pt in parts],
                        "autotuned": bool(a.autotune),
                        "parallelism": f"dp{world} (independent simulations per rank)"},

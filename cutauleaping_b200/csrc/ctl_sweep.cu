@@ -889,8 +889,11 @@ __device__ __forceinline__ Slot slot_of(unsigned char* smem, const Layout& lay, 
 // (3) groups take list entries, so every warp executes one phase only
 // (regrouping), and advance each taken simulation by a bounded amount of
 // work.  The loop ends when the queue is drained and every slot is closed.
-template <int G>
-__global__ void __launch_bounds__(256) sweep_kernel(Model m, Run run, Layout lay) {
+// MINB selects the register budget: compiled so that MINB blocks of 256
+// threads can be resident per SM (1: up to 255 registers per thread, 3: 80,
+// 4: 64, spilling to local memory as needed).  The autotuner picks it.
+template <int G, int MINB>
+__global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layout lay) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t s_cnt[2];
     const int NS = (int)(blockDim.x / G);
@@ -1147,7 +1150,7 @@ static dev::Model make_dev_model(const ctl_model* m, const DeviceCopy& d, uint32
 }
 
 struct LaunchPlan {
-    int G = 1, threads = 256, NS = 256, blocks = 1, blocks_per_sm = 1, sm_count = 1, regs = 0;
+    int G = 1, minb = 1, threads = 256, NS = 256, blocks = 1, blocks_per_sm = 1, sm_count = 1, regs = 0;
     int ssa_budget = 0, dec_budget = 0;
     size_t smem = 0;
     dev::Layout lay{};
@@ -1212,18 +1215,24 @@ static size_t slot_layout(const HostTables& t, int G, int NS, bool uniform_c, de
     return off;
 }
 
+// Register budgets compiled for every group size: minimum resident
+// 256-thread blocks per SM 1 (default), 3 or 4.
 template <int G>
-static const void* kernel_ptr() {
-    return reinterpret_cast<const void*>(&dev::sweep_kernel<G>);
+static const void* kernel_ptr(int minb) {
+    switch (minb) {
+        case 3: return reinterpret_cast<const void*>(&dev::sweep_kernel<G, 3>);
+        case 4: return reinterpret_cast<const void*>(&dev::sweep_kernel<G, 4>);
+        default: return reinterpret_cast<const void*>(&dev::sweep_kernel<G, 1>);
+    }
 }
-static const void* kernel_for(int G) {
+static const void* kernel_for(int G, int minb) {
     switch (G) {
-        case 1: return kernel_ptr<1>();
-        case 2: return kernel_ptr<2>();
-        case 4: return kernel_ptr<4>();
-        case 8: return kernel_ptr<8>();
-        case 16: return kernel_ptr<16>();
-        case 32: return kernel_ptr<32>();
+        case 1: return kernel_ptr<1>(minb);
+        case 2: return kernel_ptr<2>(minb);
+        case 4: return kernel_ptr<4>(minb);
+        case 8: return kernel_ptr<8>(minb);
+        case 16: return kernel_ptr<16>(minb);
+        case 32: return kernel_ptr<32>(minb);
     }
     return nullptr;
 }
@@ -1265,28 +1274,28 @@ static ctl_status device_attr(int dev, DevAttr& out) {
 // shared memory).  The first query raises the kernel's dynamic-memory
 // ceiling to that limit once, so every shape (cached or new) can launch.
 struct KernAttr {
-    int dev, G, regs;
+    int dev, G, minb, regs;
     size_t dyn_max;
 };
 static std::vector<KernAttr> g_kattr;
 
-static ctl_status kernel_attr(int dev, int G, KernAttr& out) {
+static ctl_status kernel_attr(int dev, int G, int minb, KernAttr& out) {
     DevAttr da;
     if (device_attr(dev, da) != CTL_OK) return CTL_ERR_CUDA;
     std::lock_guard<std::mutex> lk(g_attr_mu);
     for (const auto& a : g_kattr)
-        if (a.dev == dev && a.G == G) {
+        if (a.dev == dev && a.G == G && a.minb == minb) {
             out = a;
             return CTL_OK;
         }
-    const void* k = kernel_for(G);
+    const void* k = kernel_for(G, minb);
     cudaFuncAttributes fa;
     CTL_CUDA(cudaFuncGetAttributes(&fa, k));
     if ((size_t)da.smem_optin <= fa.sharedSizeBytes) {
         set_error("sweep kernel's static shared memory exceeds the device limit");
         return CTL_ERR_SHAPE;
     }
-    KernAttr a{dev, G, fa.numRegs, (size_t)da.smem_optin - fa.sharedSizeBytes};
+    KernAttr a{dev, G, minb, fa.numRegs, (size_t)da.smem_optin - fa.sharedSizeBytes};
     CTL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.dyn_max));
     g_kattr.push_back(a);
     out = a;
@@ -1294,25 +1303,25 @@ static ctl_status kernel_attr(int dev, int G, KernAttr& out) {
 }
 
 struct OccKey {
-    int dev, G, threads;
+    int dev, G, minb, threads;
     size_t smem;
     int bps;
 };
 static std::vector<OccKey> g_occ;
 
-static ctl_status occupancy(int dev, int G, int threads, size_t smem, int& bps, int& regs) {
+static ctl_status occupancy(int dev, int G, int minb, int threads, size_t smem, int& bps, int& regs) {
     KernAttr ka;
-    ctl_status st = kernel_attr(dev, G, ka);
+    ctl_status st = kernel_attr(dev, G, minb, ka);
     if (st != CTL_OK) return st;
     regs = ka.regs;
     std::lock_guard<std::mutex> lk(g_attr_mu);
     for (const auto& o : g_occ)
-        if (o.dev == dev && o.G == G && o.threads == threads && o.smem == smem) {
+        if (o.dev == dev && o.G == G && o.minb == minb && o.threads == threads && o.smem == smem) {
             bps = o.bps;
             return CTL_OK;
         }
-    CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel_for(G), threads, smem));
-    g_occ.push_back({dev, G, threads, smem, bps});
+    CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel_for(G, minb), threads, smem));
+    g_occ.push_back({dev, G, minb, threads, smem, bps});
     return CTL_OK;
 }
 
@@ -1359,6 +1368,7 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
             tuned_cfg.threads = e.threads;
             if (tuned_cfg.ssa_budget <= 0) tuned_cfg.ssa_budget = e.ssa_budget;
             if (tuned_cfg.dec_budget <= 0) tuned_cfg.dec_budget = e.dec_budget;
+            if (tuned_cfg.min_blocks <= 0) tuned_cfg.min_blocks = e.min_blocks;
         }
     }
     const ctl_run_cfg* cfg = &tuned_cfg;
@@ -1379,7 +1389,12 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     DevAttr da;
     if (device_attr(dev_id, da) != CTL_OK) return CTL_ERR_CUDA;
     KernAttr ka;
-    if (ctl_status st = kernel_attr(dev_id, G, ka); st != CTL_OK) return st;
+    const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : 1;
+    if (minb != 1 && minb != 3 && minb != 4) {
+        set_error("min_blocks must be 0 (library choice), 1, 3 or 4");
+        return CTL_ERR_ARG;
+    }
+    if (ctl_status st = kernel_attr(dev_id, G, minb, ka); st != CTL_OK) return st;
     const size_t smem_max = ka.dyn_max;
     const bool uni = cfg->uniform_rates != 0;
     if (cfg->threads <= 0) {
@@ -1403,7 +1418,8 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     pl.G = G;
     pl.threads = threads;
     int bps = 0, regs = 0;
-    if (ctl_status st = occupancy(dev_id, G, threads, pl.smem, bps, regs); st != CTL_OK) return st;
+    if (ctl_status st = occupancy(dev_id, G, minb, threads, pl.smem, bps, regs); st != CTL_OK) return st;
+    pl.minb = minb;
     if (bps < 1) {
         set_error("sweep kernel cannot be resident with this shape");
         return CTL_ERR_SHAPE;
@@ -1441,7 +1457,7 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     dev::Model dm = make_dev_model(m, d, cfg->flags);
     CTL_CUDA(cudaMemsetAsync(d.ctrl, 0, sizeof(uint32_t), stream));
     void* args[] = {&dm, &run, const_cast<dev::Layout*>(&pl.lay)};
-    CTL_CUDA(cudaLaunchKernel(kernel_for(pl.G), dim3((unsigned)pl.blocks), dim3((unsigned)pl.threads), args,
+    CTL_CUDA(cudaLaunchKernel(kernel_for(pl.G, pl.minb), dim3((unsigned)pl.blocks), dim3((unsigned)pl.threads), args,
                               pl.smem, stream));
     return CTL_OK;
 }
@@ -1453,6 +1469,10 @@ static ctl_status check_cfg(const ctl_run_cfg* cfg) {
     }
     if (cfg->ssa_steps == 0) {
         set_error("ssa_steps must be positive");
+        return CTL_ERR_ARG;
+    }
+    if (cfg->min_blocks != 0 && cfg->min_blocks != 1 && cfg->min_blocks != 3 && cfg->min_blocks != 4) {
+        set_error("min_blocks must be 0 (library choice), 1, 3 or 4");
         return CTL_ERR_ARG;
     }
     return CTL_OK;
@@ -1511,6 +1531,7 @@ extern "C" ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uin
     li->regs_per_thread = pl.regs;
     li->blocks_per_sm = pl.blocks_per_sm;
     li->sm_count = pl.sm_count;
+    li->min_blocks = pl.minb;
     return CTL_OK;
 }
 
@@ -1616,12 +1637,13 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
     cudaEventCreate(&e1);
     cudaError_t e = cudaMallocAsync(&dout, (size_t)k * t.ns * t.s_out * 4, s);
     if (e == cudaSuccess) e = cudaMallocAsync(&dinf, (size_t)k * sizeof(ctl_sim_info), s);
-    auto time_shape = [&](int G, int threads, int sb, int db, float& ms) -> ctl_status {
+    auto time_shape = [&](int G, int threads, int sb, int db, int mb, float& ms) -> ctl_status {
         ctl_run_cfg c = *cfg;
         c.group = G;
         c.threads = threads;
         c.ssa_budget = sb;
         c.dec_budget = db;
+        c.min_blocks = mb;
         LaunchPlan pl;
         ctl_status r = plan_launch(m, &c, k, pl);
         if (r != CTL_OK) return r;
@@ -1633,24 +1655,28 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         cudaEventElapsedTime(&ms, e0, e1);
         return CTL_OK;
     };
-    int bestG = heuristic_group(t), bestT = 256, bestS = 8, bestD = 2;
+    int bestG = heuristic_group(t), bestT = 256, bestS = 8, bestD = 2, bestM = 1;
     float best_ms = 3.4e38f;
     if (e == cudaSuccess) {
         for (int G = 1; G <= 32 && G <= t.P; G <<= 1) {  // 1. lanes per simulation
             float ms;
-            if (time_shape(G, 256, 8, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestG = G; }
+            if (time_shape(G, 256, 8, 2, 1, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestG = G; }
         }
         for (int th : {64, 128, 192}) {                   // 2. threads per block
             float ms;
-            if (th % bestG == 0 && time_shape(bestG, th, 8, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestT = th; }
+            if (th % bestG == 0 && time_shape(bestG, th, 8, 2, 1, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestT = th; }
         }
-        for (int sb : {2, 4, 16, 32}) {                    // 3. SSA steps per round
+        for (int mb : {3, 4}) {                            // 3. register budget (resident blocks)
             float ms;
-            if (time_shape(bestG, bestT, sb, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestS = sb; }
+            if (time_shape(bestG, bestT, 8, 2, mb, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestM = mb; }
         }
-        for (int db : {1, 4, 8}) {                         // 4. decisions per round
+        for (int sb : {2, 4, 16, 32}) {                    // 4. SSA steps per round
             float ms;
-            if (time_shape(bestG, bestT, bestS, db, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestD = db; }
+            if (time_shape(bestG, bestT, sb, 2, bestM, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestS = sb; }
+        }
+        for (int db : {1, 4, 8}) {                         // 5. decisions per round
+            float ms;
+            if (time_shape(bestG, bestT, bestS, db, bestM, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestD = db; }
         }
     }
     if (dout) cudaFreeAsync(dout, s);
@@ -1667,15 +1693,16 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         bool found = false;
         for (auto& x : m->tuned)
             if (x.device == cfg->device && x.nbucket == nb && x.uniform == uni && x.flags == cfg->flags) {
-                x.group = bestG; x.threads = bestT; x.ssa_budget = bestS; x.dec_budget = bestD;
+                x.group = bestG; x.threads = bestT; x.ssa_budget = bestS; x.dec_budget = bestD; x.min_blocks = bestM;
                 found = true;
             }
-        if (!found) m->tuned.push_back({cfg->device, nb, uni, cfg->flags, bestG, bestT, bestS, bestD});
+        if (!found) m->tuned.push_back({cfg->device, nb, uni, cfg->flags, bestG, bestT, bestS, bestD, bestM});
     }
     if (best) {
         ctl_run_cfg c = *cfg;
         c.group = 0;
         c.threads = 0;
+        c.min_blocks = 0;
         return ctl_launch_query(m, &c, n, best);
     }
     return CTL_OK;

@@ -91,7 +91,9 @@ typedef struct {
                              ctl_run detects this itself, device calls take it as given */
     int32_t ssa_budget;   /* SSA steps per simulation and scheduling round (0 = 8)     */
     int32_t dec_budget;   /* leap decisions per simulation and round (0 = 2)           */
-    int32_t reserved;
+    int32_t min_blocks;   /* register budget: kernel variant compiled for this many resident
+                             256-thread blocks per SM (1: up to 255 registers per thread,
+                             3: 80, 4: 64); 0 = library choice (autotuned, else 1)    */
 } ctl_run_cfg;
 
 typedef struct {
@@ -104,6 +106,7 @@ typedef struct {
 typedef struct {
     int32_t group, threads, blocks, slots_per_block;
     int32_t smem_bytes, regs_per_thread, blocks_per_sm, sm_count;
+    int32_t min_blocks;   /* register budget of the kernel variant (ctl_run_cfg.min_blocks) */
 } ctl_launch_info;
 
 /* ---- errors ------------------------------------------------------------ */

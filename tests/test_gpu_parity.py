@@ -56,6 +56,20 @@ def test_launch_shape_invariance(name, net):
             assert same_info(info, ref_info) is None, f"{name} G={G} threads={threads}"
 
 
+@pytest.mark.parametrize("name,net", NETS, ids=[n for n, _ in NETS])
+def test_register_budget_invariance(name, net):
+    """The register-budget variants (min_blocks 3 and 4, which spill to local
+    memory) run the same arithmetic: identical to the oracle."""
+    out_o, info_o = oracle_run(net, seed=31)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    for mb in (3, 4):
+        for G in (1, 8):
+            out, info = m.run(net.X0, net.c, seed=31, group=G, min_blocks=mb)
+            assert np.array_equal(out, out_o), f"{name} G={G} min_blocks={mb}"
+            assert same_info(info, info_o) is None, f"{name} G={G} min_blocks={mb}"
+            assert m.launch_info(net.n, group=G, min_blocks=mb).min_blocks == mb
+
+
 def test_sim_base_selects_rows_of_a_larger_run():
     """The reference's `offset` shards rows; with sim_base the shard reproduces
     the same simulations a single large run produces."""

@@ -159,3 +159,14 @@ def test_cli_usage_and_early_exit_codes(tmp_path):
     folder2 = _folder(tmp_path / "x", MX_0=None)
     p = _cli(folder2, 2, 2, 0, 0, tmp_path / "out", "pref", 0, 0, 0)
     assert p.returncode == 256 - 6
+
+
+@pytest.mark.parametrize("kw", [{"min_blocks": 2}, {"min_blocks": 5}, {"ssa_steps": 0}])
+def test_run_cfg_rejected_before_any_device_work(kw):
+    """Invalid run configurations fail with CTL_ERR_ARG in host code, before
+    the library selects or touches a device."""
+    net = inputs.schlogl(4, samples=5, t_end=0.1)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    with pytest.raises(ctl.CtlError) as e:
+        m.run(net.X0, net.c, **kw)
+    assert e.value.status == ctl.ERR_ARG
