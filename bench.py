@@ -179,6 +179,38 @@ def cpu_reference_segments(segs, steps, warmup):
     return tot_n / tot_t, tot_f / tot_t, {"cores": meta["cores"], "sample": "; ".join(samples)}
 
 
+def screen_roofline(p, net, sc, n_cand):
+    """Tensor roofline of the fused screening kernel (ctl_mlp_screen): n_cand
+    candidates x ns instants rows, 2 * (64*256 + 3*256*256 + 256*out_w)
+    FLOPs per row, CUDA events on the launching stream over 10 launches after
+    3 warm-ups; peak = the measured burst BF16 GEMM rate."""
+    import torch
+    from cutauleaping_b200 import surrogate as sg
+    rng = np.random.default_rng(12)
+    th = torch.as_tensor(rng.uniform(p.log_lo, p.log_hi, size=(n_cand, len(p.unknown))), dtype=torch.float32,
+                         device="cuda")
+    tgt = p.target.astype(np.float32)
+    for _ in range(3):
+        sg.screen(net, th, p.tvec, tgt, sc)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    reps = 10
+    for _ in range(reps):
+        sg.screen(net, th, p.tvec, tgt, sc)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    flops = float(n_cand * len(p.tvec)) * 2.0 * (64 * 256 + 3 * 256 * 256 + 256 * net.out_w)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    peak = float(peaks["bf16_tflops"])
+    ach = flops / (ms * 1e-3) / 1e12
+    return {"bound": "tensor", "kernel": "screen_kernel (fused 5-layer MLP + fitness)", "achieved": ach,
+            "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+            "launch_ms": ms, "rows_per_launch": n_cand * len(p.tvec),
+            "peak_source": "MEASURED_PEAKS.json bf16_tflops (measured, burst)"}
+
+
 def bench_config5(a):
     """Surrogate-screened parameter estimation against plain-simulator search.
 
@@ -213,13 +245,17 @@ def bench_config5(a):
     net, sc = fs.train_surrogate(p, theta, traj, epochs=2, batch=16384)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0 - t_data
-    ts, ss, surr_ok, sh = run_until("surrogate", t_data + t_train, screen=screen, keep_frac=0.01, net=net, sc=sc)
+    ts, ss, surr_ok, sh = run_until("surrogate", t_data + t_train, screen=screen, keep_frac=0.01, net=net, sc=sc,
+                                    inner=a.inner)
+    scr = screen_roofline(p, net, sc, n_cand=200_000)
     print(json.dumps({
         "metric": METRIC, "config": {"workload": "surrogate-screened parameter estimation: 32x64 network "
                                                  "(generator seed 1), 8 unknown rate constants, target = mean "
                                                  f"of {n_rep} simulations at 50 instants", "full_size": full,
                                      "n_rep": n_rep, "training_trajectories": n_traj, "screened_per_gen": screen,
+                                     "surrogate_iterations_per_gen": a.inner,
                                      "resimulated_per_gen": pop, "max_generations": max_gen},
+        "roofline": scr, "gpu_launches": None,
         "value": 1.0 / ts, "unit": "fits/s (surrogate-screened)", "plain_fits_per_s": 1.0 / tp,
         "speedup_vs_plain": tp / ts, "speedup_is_lower_bound": not plain_ok, "surrogate_reached": surr_ok,
         "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
@@ -241,11 +277,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5])
     ap.add_argument("--full", action="store_true", help="config 5 at the configured sizes")
+    ap.add_argument("--inner", type=int, default=1, help="config 5: surrogate-only iterations per generation")
     ap.add_argument("--sims", type=int, default=None, help="simulations per GPU (default: config's)")
     ap.add_argument("--group", type=int, default=0, help="lanes per simulation (0 = library choice)")
     ap.add_argument("--threads", type=int, default=0, help="threads per block (0 = library choice)")
     ap.add_argument("--min-blocks", type=int, default=0,
                     help="register budget of the sweep kernel: 1, 3 or 4 resident blocks (0 = library choice)")
+    ap.add_argument("--sched", type=int, default=0,
+                    help="scheduling: 1 block regrouping rounds, 2 warp-local (0 = library choice)")
     ap.add_argument("--autotune", action="store_true", help="measure launch shapes before timing")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -296,7 +335,7 @@ def main():
         model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
         n = net.n
         cfg = ctl.run_cfg(seed=1 + si, sim_base=rank * n, device=local, group=a.group, threads=a.threads,
-                          min_blocks=a.min_blocks, uniform_rates=int(bool((net.c == net.c[0]).all())))
+                          min_blocks=a.min_blocks, sched=a.sched, uniform_rates=int(bool((net.c == net.c[0]).all())))
         X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).to(dev)
         c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).to(dev)
         out = torch.empty((n, model.ns, model.s_out), dtype=torch.int32, device=dev)
@@ -431,7 +470,7 @@ def main():
                        "launch": [{"group": pt["li"].group, "threads": pt["li"].threads,
                                    "blocks": pt["li"].blocks, "slots_per_block": pt["li"].slots_per_block,
                                    "smem_bytes": pt["li"].smem_bytes, "regs": pt["li"].regs_per_thread,
-                                   "min_blocks": pt["li"].min_blocks,
+                                   "min_blocks": pt["li"].min_blocks, "sched": pt["li"].sched,
                                    "blocks_per_sm": pt["li"].blocks_per_sm} for pt in parts],
                        "autotuned": bool(a.autotune),
                        "parallelism": f"dp{world} (independent simulations per rank)"},

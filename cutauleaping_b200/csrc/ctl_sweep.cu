@@ -83,6 +83,7 @@ struct Run {
     uint32_t ssa_steps, flags, max_steps, sim_base, n;
     uint32_t uniform_c;              // all simulations share row 0 of c
     uint32_t ssa_budget, dec_budget; // work per slot and round (SSA steps / decisions)
+    uint32_t warp_local;             // 1: warp-local scheduling (no block rounds)
     const int32_t* __restrict__ X0;  // [n][S]
     const float* __restrict__ c;     // [n][R]
     uint32_t* __restrict__ out;      // [n][ns][s_out]
@@ -927,6 +928,53 @@ __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layo
     __syncthreads();
     const uint32_t ns = (uint32_t)m.ns;
     const size_t sim_stride = (size_t)ns * (size_t)m.s_out;
+    if (run.warp_local) {
+        // Warp-local scheduling: every group keeps its own slot and its
+        // simulation's scalars in registers; the groups of a warp step in
+        // lockstep per phase and no block-wide barrier is taken, so a long
+        // leap decision in one warp never holds up the others.
+        const Slot sl = slot_of<G>(smem, lay, gi, NS, uni);
+        Sim st;
+        bool live = false, closed = false;
+        uint32_t* out = run.out;
+        for (;;) {
+            if (!live && !closed) {
+                uint32_t sim = 0;
+                if (g.lane == 0) sim = atomicAdd(run.queue, 1u);
+                sim = g.bcast(sim);
+                if (sim >= run.n) {
+                    closed = true;
+                } else {
+                    init_sim<G>(g, m, run, sl, st, sim);
+                    live = true;
+                    out = run.out + (size_t)st.sim * sim_stride;
+                }
+            }
+            if (__all_sync(0xffffffffu, closed)) break;
+            const bool is_ssa = live && st.in_ssa, is_dec = live && !st.in_ssa;
+            const uint32_t ssa_mask = __ballot_sync(0xffffffffu, is_ssa);
+            const uint32_t dec_mask = __ballot_sync(0xffffffffu, is_dec);
+            int res = CONT;
+            if (is_ssa) {
+                for (uint32_t b = 0; b < run.ssa_budget; b++) {
+                    const bool act = res == CONT && st.in_ssa;
+                    if (!__any_sync(ssa_mask, act)) break;
+                    if (act) res = ssa_step<G>(g, m, run, sl, st, out);
+                }
+            } else if (is_dec) {
+                for (uint32_t b = 0; b < run.dec_budget; b++) {
+                    const bool act = res == CONT && !st.in_ssa;
+                    if (!__any_sync(dec_mask, act)) break;
+                    if (act) res = decide_step<G>(g, m, run, sl, st, out);
+                }
+            }
+            if (live && res == DONE) {
+                finish_sim<G>(g, m, run, st, out);
+                live = false;
+            }
+        }
+        return;
+    }
     for (;;) {
         if (phase[gi] == PH_EMPTY) {
             uint32_t sim = 0;
@@ -1150,7 +1198,7 @@ static dev::Model make_dev_model(const ctl_model* m, const DeviceCopy& d, uint32
 }
 
 struct LaunchPlan {
-    int G = 1, minb = 1, threads = 256, NS = 256, blocks = 1, blocks_per_sm = 1, sm_count = 1, regs = 0;
+    int G = 1, minb = 1, sched = 1, threads = 256, NS = 256, blocks = 1, blocks_per_sm = 1, sm_count = 1, regs = 0;
     int ssa_budget = 0, dec_budget = 0;
     size_t smem = 0;
     dev::Layout lay{};
@@ -1369,11 +1417,13 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
             if (tuned_cfg.ssa_budget <= 0) tuned_cfg.ssa_budget = e.ssa_budget;
             if (tuned_cfg.dec_budget <= 0) tuned_cfg.dec_budget = e.dec_budget;
             if (tuned_cfg.min_blocks <= 0) tuned_cfg.min_blocks = e.min_blocks;
+            if (tuned_cfg.sched <= 0) tuned_cfg.sched = e.sched;
         }
     }
     const ctl_run_cfg* cfg = &tuned_cfg;
     pl.ssa_budget = cfg->ssa_budget;
     pl.dec_budget = cfg->dec_budget;
+    pl.sched = cfg->sched > 0 ? cfg->sched : 1;
     int G = cfg->group > 0 ? cfg->group : heuristic_group(t);
     if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32) {
         set_error("group must be one of 1, 2, 4, 8, 16, 32");
@@ -1449,6 +1499,7 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.uniform_c = cfg->uniform_rates != 0;
     run.ssa_budget = pl.ssa_budget > 0 ? (uint32_t)pl.ssa_budget : 8u;
     run.dec_budget = pl.dec_budget > 0 ? (uint32_t)pl.dec_budget : 2u;
+    run.warp_local = pl.sched == 2 ? 1u : 0u;
     run.X0 = dX0;
     run.c = dc;
     run.out = dout;
@@ -1473,6 +1524,10 @@ static ctl_status check_cfg(const ctl_run_cfg* cfg) {
     }
     if (cfg->min_blocks != 0 && cfg->min_blocks != 1 && cfg->min_blocks != 3 && cfg->min_blocks != 4) {
         set_error("min_blocks must be 0 (library choice), 1, 3 or 4");
+        return CTL_ERR_ARG;
+    }
+    if (cfg->sched < 0 || cfg->sched > 2) {
+        set_error("sched must be 0 (library choice), 1 (block regrouping) or 2 (warp-local)");
         return CTL_ERR_ARG;
     }
     return CTL_OK;
@@ -1532,6 +1587,7 @@ extern "C" ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uin
     li->blocks_per_sm = pl.blocks_per_sm;
     li->sm_count = pl.sm_count;
     li->min_blocks = pl.minb;
+    li->sched = pl.sched;
     return CTL_OK;
 }
 
@@ -1637,13 +1693,14 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
     cudaEventCreate(&e1);
     cudaError_t e = cudaMallocAsync(&dout, (size_t)k * t.ns * t.s_out * 4, s);
     if (e == cudaSuccess) e = cudaMallocAsync(&dinf, (size_t)k * sizeof(ctl_sim_info), s);
-    auto time_shape = [&](int G, int threads, int sb, int db, int mb, float& ms) -> ctl_status {
+    auto time_shape = [&](int G, int threads, int sb, int db, int mb, int sc, float& ms) -> ctl_status {
         ctl_run_cfg c = *cfg;
         c.group = G;
         c.threads = threads;
         c.ssa_budget = sb;
         c.dec_budget = db;
         c.min_blocks = mb;
+        c.sched = sc;
         LaunchPlan pl;
         ctl_status r = plan_launch(m, &c, k, pl);
         if (r != CTL_OK) return r;
@@ -1655,28 +1712,38 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         cudaEventElapsedTime(&ms, e0, e1);
         return CTL_OK;
     };
-    int bestG = heuristic_group(t), bestT = 256, bestS = 8, bestD = 2, bestM = 1;
+    int bestG = heuristic_group(t), bestT = 256, bestS = 8, bestD = 2, bestM = 1, bestC = 1;
     float best_ms = 3.4e38f;
     if (e == cudaSuccess) {
         for (int G = 1; G <= 32 && G <= t.P; G <<= 1) {  // 1. lanes per simulation
             float ms;
-            if (time_shape(G, 256, 8, 2, 1, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestG = G; }
+            if (time_shape(G, 256, 8, 2, 1, 1, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestG = G; }
         }
         for (int th : {64, 128, 192}) {                   // 2. threads per block
             float ms;
-            if (th % bestG == 0 && time_shape(bestG, th, 8, 2, 1, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestT = th; }
+            if (th % bestG == 0 && time_shape(bestG, th, 8, 2, 1, 1, ms) == CTL_OK && ms < best_ms) {
+                best_ms = ms;
+                bestT = th;
+            }
         }
-        for (int mb : {3, 4}) {                            // 3. register budget (resident blocks)
+        {                                                  // 3. scheduling: warp-local vs block rounds
             float ms;
-            if (time_shape(bestG, bestT, 8, 2, mb, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestM = mb; }
+            if (time_shape(bestG, bestT, 8, 2, 1, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestC = 2; }
         }
-        for (int sb : {2, 4, 16, 32}) {                    // 4. SSA steps per round
+        for (int mb : {3, 4}) {                            // 4. register budget (resident blocks)
             float ms;
-            if (time_shape(bestG, bestT, sb, 2, bestM, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestS = sb; }
+            if (time_shape(bestG, bestT, 8, 2, mb, bestC, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestM = mb; }
         }
-        for (int db : {1, 4, 8}) {                         // 5. decisions per round
+        for (int sb : {2, 4, 16, 32}) {                    // 5. SSA steps per round
             float ms;
-            if (time_shape(bestG, bestT, bestS, db, bestM, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestD = db; }
+            if (time_shape(bestG, bestT, sb, 2, bestM, bestC, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestS = sb; }
+        }
+        for (int db : {1, 4, 8}) {                         // 6. decisions per round
+            float ms;
+            if (time_shape(bestG, bestT, bestS, db, bestM, bestC, ms) == CTL_OK && ms < best_ms) {
+                best_ms = ms;
+                bestD = db;
+            }
         }
     }
     if (dout) cudaFreeAsync(dout, s);
@@ -1694,15 +1761,17 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         for (auto& x : m->tuned)
             if (x.device == cfg->device && x.nbucket == nb && x.uniform == uni && x.flags == cfg->flags) {
                 x.group = bestG; x.threads = bestT; x.ssa_budget = bestS; x.dec_budget = bestD; x.min_blocks = bestM;
+                x.sched = bestC;
                 found = true;
             }
-        if (!found) m->tuned.push_back({cfg->device, nb, uni, cfg->flags, bestG, bestT, bestS, bestD, bestM});
+        if (!found) m->tuned.push_back({cfg->device, nb, uni, cfg->flags, bestG, bestT, bestS, bestD, bestM, bestC});
     }
     if (best) {
         ctl_run_cfg c = *cfg;
         c.group = 0;
         c.threads = 0;
         c.min_blocks = 0;
+        c.sched = 0;
         return ctl_launch_query(m, &c, n, best);
     }
     return CTL_OK;

@@ -94,6 +94,8 @@ typedef struct {
     int32_t min_blocks;   /* register budget: kernel variant compiled for this many resident
                              256-thread blocks per SM (1: up to 255 registers per thread,
                              3: 80, 4: 64); 0 = library choice (autotuned, else 1)    */
+    int32_t sched;        /* scheduling: 1 = block rounds regrouping simulations by phase,
+                             2 = warp-local (no block barriers); 0 = library choice   */
 } ctl_run_cfg;
 
 typedef struct {
@@ -107,6 +109,7 @@ typedef struct {
     int32_t group, threads, blocks, slots_per_block;
     int32_t smem_bytes, regs_per_thread, blocks_per_sm, sm_count;
     int32_t min_blocks;   /* register budget of the kernel variant (ctl_run_cfg.min_blocks) */
+    int32_t sched;        /* scheduling mode (ctl_run_cfg.sched) */
 } ctl_launch_info;
 
 /* ---- errors ------------------------------------------------------------ */

@@ -70,6 +70,20 @@ def test_register_budget_invariance(name, net):
             assert m.launch_info(net.n, group=G, min_blocks=mb).min_blocks == mb
 
 
+@pytest.mark.parametrize("name,net", NETS, ids=[n for n, _ in NETS])
+def test_warp_local_scheduling_invariance(name, net):
+    """Warp-local scheduling (no block rounds) changes only which warp runs a
+    simulation when: identical to the oracle for every group size."""
+    out_o, info_o = oracle_run(net, seed=47)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    for G in (1, 4, 32):
+        for threads in (32, 256):
+            out, info = m.run(net.X0, net.c, seed=47, group=G, threads=threads, sched=2, ssa_budget=3)
+            assert np.array_equal(out, out_o), f"{name} G={G} threads={threads}"
+            assert same_info(info, info_o) is None, f"{name} G={G} threads={threads}"
+    assert m.launch_info(net.n, sched=2).sched == 2
+
+
 def test_sim_base_selects_rows_of_a_larger_run():
     """The reference's `offset` shards rows; with sim_base the shard reproduces
     the same simulations a single large run produces."""
