@@ -891,8 +891,8 @@ __device__ __forceinline__ Slot slot_of(unsigned char* smem, const Layout& lay, 
 // (regrouping), and advance each taken simulation by a bounded amount of
 // work.  The loop ends when the queue is drained and every slot is closed.
 // MINB selects the register budget: compiled so that MINB blocks of 256
-// threads can be resident per SM (1: up to 255 registers per thread, 3: 80,
-// 4: 64, spilling to local memory as needed).  The autotuner picks it.
+// threads can be resident per SM (2: up to 128 registers per thread, 3: 80,
+// 4: 64, spilling to local memory as needed).
 template <int G, int MINB>
 __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layout lay) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1264,13 +1264,13 @@ static size_t slot_layout(const HostTables& t, int G, int NS, bool uniform_c, de
 }
 
 // Register budgets compiled for every group size: minimum resident
-// 256-thread blocks per SM 1 (default), 3 or 4.
+// 256-thread blocks per SM 2, 3 or 4.
 template <int G>
 static const void* kernel_ptr(int minb) {
     switch (minb) {
         case 3: return reinterpret_cast<const void*>(&dev::sweep_kernel<G, 3>);
         case 4: return reinterpret_cast<const void*>(&dev::sweep_kernel<G, 4>);
-        default: return reinterpret_cast<const void*>(&dev::sweep_kernel<G, 1>);
+        default: return reinterpret_cast<const void*>(&dev::sweep_kernel<G, 2>);
     }
 }
 static const void* kernel_for(int G, int minb) {
@@ -1439,14 +1439,16 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     DevAttr da;
     if (device_attr(dev_id, da) != CTL_OK) return CTL_ERR_CUDA;
     KernAttr ka;
-    const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : 1;
-    if (minb != 1 && minb != 3 && minb != 4) {
-        set_error("min_blocks must be 0 (library choice), 1, 3 or 4");
-        return CTL_ERR_ARG;
+    const bool uni = cfg->uniform_rates != 0;
+    // Register budget: as many resident blocks as the slot memory of a full
+    // 256-thread block allows (2 or 3; 4 only when chosen or tuned).
+    int minb = cfg->min_blocks;
+    if (minb <= 0) {
+        const size_t full = slot_layout(t, G, 256 / G, uni, pl.lay);
+        minb = 3 * (full + 1024) <= (size_t)da.smem_optin + 1024 ? 3 : 2;
     }
     if (ctl_status st = kernel_attr(dev_id, G, minb, ka); st != CTL_OK) return st;
     const size_t smem_max = ka.dyn_max;
-    const bool uni = cfg->uniform_rates != 0;
     if (cfg->threads <= 0) {
         while (threads > 32 && (uint64_t)n * G < (uint64_t)threads * da.sm_count) threads -= 32;
     }
@@ -1522,8 +1524,8 @@ static ctl_status check_cfg(const ctl_run_cfg* cfg) {
         set_error("ssa_steps must be positive");
         return CTL_ERR_ARG;
     }
-    if (cfg->min_blocks != 0 && cfg->min_blocks != 1 && cfg->min_blocks != 3 && cfg->min_blocks != 4) {
-        set_error("min_blocks must be 0 (library choice), 1, 3 or 4");
+    if (cfg->min_blocks != 0 && (cfg->min_blocks < 2 || cfg->min_blocks > 4)) {
+        set_error("min_blocks must be 0 (library choice), 2, 3 or 4");
         return CTL_ERR_ARG;
     }
     if (cfg->sched < 0 || cfg->sched > 2) {
@@ -1712,23 +1714,23 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         cudaEventElapsedTime(&ms, e0, e1);
         return CTL_OK;
     };
-    int bestG = heuristic_group(t), bestT = 256, bestS = 8, bestD = 2, bestM = 1, bestC = 1;
+    int bestG = heuristic_group(t), bestT = 256, bestS = 8, bestD = 2, bestM = 2, bestC = 1;
     float best_ms = 3.4e38f;
     if (e == cudaSuccess) {
         for (int G = 1; G <= 32 && G <= t.P; G <<= 1) {  // 1. lanes per simulation
             float ms;
-            if (time_shape(G, 256, 8, 2, 1, 1, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestG = G; }
+            if (time_shape(G, 256, 8, 2, 2, 1, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestG = G; }
         }
         for (int th : {64, 128, 192}) {                   // 2. threads per block
             float ms;
-            if (th % bestG == 0 && time_shape(bestG, th, 8, 2, 1, 1, ms) == CTL_OK && ms < best_ms) {
+            if (th % bestG == 0 && time_shape(bestG, th, 8, 2, 2, 1, ms) == CTL_OK && ms < best_ms) {
                 best_ms = ms;
                 bestT = th;
             }
         }
         {                                                  // 3. scheduling: warp-local vs block rounds
             float ms;
-            if (time_shape(bestG, bestT, 8, 2, 1, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestC = 2; }
+            if (time_shape(bestG, bestT, 8, 2, 2, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestC = 2; }
         }
         for (int mb : {3, 4}) {                            // 4. register budget (resident blocks)
             float ms;

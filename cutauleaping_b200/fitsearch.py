@@ -101,14 +101,17 @@ def simulate(p: FitProblem, theta_log, n_rep, *, seed, sim_base=0):
     return _sweep(p, np.asarray(theta_log), n_rep, seed, sim_base, torch).cpu().numpy().view(np.uint32)
 
 
-def true_fitness(p: FitProblem, theta_log, *, seed, sim_base=0, chunk=256):
-    """Reference fitness of each candidate from n_rep simulations, on the device."""
+def true_fitness(p: FitProblem, theta_log, *, seed, sim_base=0, chunk=256, keep_reps=0):
+    """Reference fitness of each candidate from n_rep simulations, on the
+    device.  With keep_reps > 0 also returns the first keep_reps trajectories
+    of every candidate (device tensor [n*keep_reps][ns][S], candidate-major)."""
     import torch
     L = lib()
     theta_log = np.asarray(theta_log)
     n = theta_log.shape[0]
     tgt = torch.as_tensor(p.target.astype(np.uint32).view(np.int32).reshape(-1), device="cuda")
     fit = np.empty(n)
+    kept = []
     for a in range(0, n, chunk):
         th = theta_log[a:a + chunk]
         k = th.shape[0]
@@ -121,6 +124,11 @@ def true_fitness(p: FitProblem, theta_log, *, seed, sim_base=0, chunk=256):
         if st != OK:
             raise CtlError(st, "ctl_fitness_device")
         fit[a:a + k] = f[:k].cpu().numpy()
+        if keep_reps:
+            r = min(keep_reps, p.n_rep)
+            kept.append(out.view(k, p.n_rep, len(p.tvec), p.S)[:, :r].reshape(k * r, len(p.tvec), p.S).clone())
+    if keep_reps:
+        return fit, torch.cat(kept)
     return fit
 
 
@@ -137,20 +145,28 @@ def training_data(p: FitProblem, n_traj, *, seed=5, sim_seed=91):
     return torch.as_tensor(theta, dtype=torch.float32, device="cuda"), out
 
 
-def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-3, seed=0, log=None):
+def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-3, seed=0, log=None,
+                    net=None, sc=None, steps=None, cosine=True):
     """Fit the MLP to (theta, t) -> counts of single trajectories (Gaussian
-    NLL: the network learns the ensemble mean and log-variance)."""
+    NLL: the network learns the ensemble mean and log-variance).  With `net`
+    and `sc` given, continues training that network (fine-tuning) with its
+    output scaling unchanged."""
     import torch
     n, ns, S = traj.shape
     y = traj.to(torch.float32)
-    y_mean = y.mean(dim=(0, 1))
-    y_std = y.std(dim=(0, 1)).clamp_min(1.0)
-    sc = sg.Scaling(p.log_lo, p.log_hi, float(p.tvec[-1]), y_mean.cpu().numpy(), y_std.cpu().numpy())
+    if sc is None:
+        y_mean = y.mean(dim=(0, 1))
+        y_std = y.std(dim=(0, 1)).clamp_min(1.0)
+        sc = sg.Scaling(p.log_lo, p.log_hi, float(p.tvec[-1]), y_mean.cpu().numpy(), y_std.cpu().numpy())
+    else:
+        y_mean = torch.as_tensor(sc.y_mean, dtype=torch.float32, device="cuda")
+        y_std = torch.as_tensor(sc.y_std, dtype=torch.float32, device="cuda")
     tv = torch.as_tensor(p.tvec, dtype=torch.float32, device="cuda")
-    net = sg.MLP(S, seed=seed)
+    if net is None:
+        net = sg.MLP(S, seed=seed)
     total = n * ns
-    steps = max(1, (epochs * total) // batch)
-    g = torch.Generator(device="cuda").manual_seed(seed)
+    steps = steps or max(1, (epochs * total) // batch)
+    g = torch.Generator(device="cuda").manual_seed(seed + net.step_count)
     hist = []
     for it in range(steps):
         idx = torch.randint(0, total, (batch,), device="cuda", generator=g)
@@ -159,7 +175,7 @@ def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-
         tgt = (y[si, ti] - y_mean) / y_std
         out = net.forward(X)
         loss, dW, db = net.backward(out, tgt)
-        rate = lr * 0.5 * (1 + math.cos(math.pi * it / steps))
+        rate = lr * 0.5 * (1 + math.cos(math.pi * it / steps)) if cosine else lr
         net.adam(dW, db, lr=rate)
         if log is not None and (it % 200 == 0 or it == steps - 1):
             hist.append((it, loss.item() / (batch * S)))
@@ -211,7 +227,8 @@ def predicted_fitness_layers(p: FitProblem, net, sc, theta_log, *, chunk=65536):
 # ---------------------------------------------------------------------------
 
 def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_frac=0.01, net=None,
-        sc=None, seed=0, sim_seed=1000, time_limit=None, stop_at=None, inner=1):
+        sc=None, seed=0, sim_seed=1000, time_limit=None, stop_at=None, inner=1, explore_frac=0.0,
+        finetune_steps=0, finetune_reps=8, finetune_lr=5e-4, finetune_batch=8192):
     """Cross-entropy search in log-parameter space.
 
     mode 'plain' simulates every one of `pop` candidates per generation.
@@ -219,10 +236,15 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
     iterations from the current proposal (each screens `screen` candidates
     and refits the proposal to the best `elite` fraction by predicted
     fitness; the last one keeps its screened set), then re-simulates the best
-    max(pop, keep_frac * screen) screened candidates and refits the proposal
-    to their best by true fitness.  Every candidate whose fitness is reported
-    was simulated.  Returns a list of (wall seconds, simulations so far, best
+    max(pop, keep_frac * screen) screened candidates -- of which a fraction
+    `explore_frac` is replaced by unscreened draws from the proposal -- and
+    refits the proposal to their best by true fitness.  With
+    finetune_steps > 0 the surrogate is then fine-tuned on `finetune_reps`
+    of the trajectories just simulated per candidate, so its error shrinks
+    where the search is.  Every candidate whose fitness is reported was
+    simulated.  Returns a list of (wall seconds, simulations so far, best
     true fitness, best theta), one entry per generation."""
+    import torch
     rng = np.random.default_rng(seed)
     d = len(p.unknown)
     mu = (p.log_lo + p.log_hi) / 2
@@ -243,8 +265,15 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
                     el = big[order[: max(2, int(elite * keep_frac * screen))]]
                     mu = el.mean(0)
                     sd = np.maximum(el.std(0), floor)
-            cand = big[order[: max(pop, int(keep_frac * screen))]]
-        f = true_fitness(p, cand, seed=sim_seed + gen, sim_base=0)
+            nk = max(pop, int(keep_frac * screen))
+            nx = int(explore_frac * nk)
+            cand = big[order[: nk - nx]]
+            if nx:
+                cand = np.concatenate([cand, np.clip(rng.normal(mu, sd, size=(nx, d)), p.log_lo, p.log_hi)])
+        if mode != "plain" and finetune_steps:
+            f, traj = true_fitness(p, cand, seed=sim_seed + gen, sim_base=0, keep_reps=finetune_reps)
+        else:
+            f = true_fitness(p, cand, seed=sim_seed + gen, sim_base=0)
         sims += len(cand) * p.n_rep
         order = np.argsort(f)
         if f[order[0]] < best_f:
@@ -258,4 +287,9 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
             break
         if stop_at is not None and best_f <= stop_at:
             break
+        if mode != "plain" and finetune_steps:
+            th = torch.as_tensor(np.repeat(cand, min(finetune_reps, p.n_rep), axis=0), dtype=torch.float32,
+                                 device="cuda")
+            train_surrogate(p, th, traj, net=net, sc=sc, steps=finetune_steps, lr=finetune_lr,
+                            batch=finetune_batch, cosine=False)
     return hist

@@ -92,8 +92,9 @@ typedef struct {
     int32_t ssa_budget;   /* SSA steps per simulation and scheduling round (0 = 8)     */
     int32_t dec_budget;   /* leap decisions per simulation and round (0 = 2)           */
     int32_t min_blocks;   /* register budget: kernel variant compiled for this many resident
-                             256-thread blocks per SM (1: up to 255 registers per thread,
-                             3: 80, 4: 64); 0 = library choice (autotuned, else 1)    */
+                             256-thread blocks per SM (2: up to 128 registers per thread,
+                             3: 80, 4: 64); 0 = library choice (autotuned, else 3 when
+                             three full blocks' slots fit in shared memory, else 2)   */
     int32_t sched;        /* scheduling: 1 = block rounds regrouping simulations by phase,
                              2 = warp-local (no block barriers); 0 = library choice   */
 } ctl_run_cfg;
