@@ -134,9 +134,18 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
     for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU through the logistic function written with the hardware tanh:
+// sigmoid(z) = 0.5 + 0.5 tanh(z / 2), one MUFU operation per element
+// (tanh.approx.f32, relative error about 2^-11, below the BF16 rounding that
+// follows).  Training and screening use the same form.
+__device__ __forceinline__ float sigm(float z) {
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
+    return fmaf(0.5f, t, 0.5f);
+}
+__device__ __forceinline__ float silu(float z) { return z * sigm(z); }
 __device__ __forceinline__ float silu_grad(float z) {
-    const float s = 1.0f / (1.0f + __expf(-z));
+    const float s = sigm(z);
     return s * (1.0f + z * (1.0f - s));
 }
 
@@ -345,7 +354,7 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
 //   * warp 5 (MMA): one thread issues tcgen05.mma (M = 128, N = layer width,
 //     K = 16) from the activation tile and the weight stage into TMEM.
 // Two CTAs share an SM, so one CTA's epilogue overlaps the other's MMAs.
-constexpr int SC_BK = 32, SC_STAGES = 3, SC_THREADS = 192, SC_HID = 256, SC_LAYERS = 5;
+constexpr int SC_BK = 32, SC_STAGES = 3, SC_THREADS = 320, SC_EPI = 256, SC_HID = 256, SC_LAYERS = 5;
 constexpr int SC_A_BYTES = 128 * SC_HID * 2;
 constexpr int SC_STAGE_BYTES = SC_HID * SC_BK * 2;
 
@@ -382,6 +391,20 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     uint32_t r[16];
     asm volatile(
@@ -394,15 +417,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
-// Named barrier over the 128 epilogue threads (warps 0-3), and the same
+// Named barrier over the 256 epilogue threads (warps 0-7), and the same
 // barrier as a vote: true when every epilogue thread passes true.
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 __device__ __forceinline__ bool epi_all(bool v) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred a, b;\n\t"
         "setp.ne.u32 a, %1, 0;\n\t"
-        "bar.red.and.pred b, 1, 128, a;\n\t"
+        "bar.red.and.pred b, 1, 256, a;\n\t"
         "selp.u32 %0, 1, 0, b;\n\t}"
         : "=r"(r)
         : "r"((uint32_t)v)
@@ -420,34 +443,34 @@ __device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
     return (uint32_t)__bfloat16_as_ushort(x) | ((uint32_t)__bfloat16_as_ushort(y) << 16);
 }
 
-// Layer-0 input of row r of the tile: scaled log parameters in [-1, 1],
-// scaled time, zeros (the same FP32 operations as surrogate.make_inputs).
-__device__ void sc_build_input(const Screen& p, uint8_t* A, int r, uint32_t row) {
-    float x[64];
+// Layer-0 input columns [32h, 32h + 32) of row r of the tile: scaled log
+// parameters in [-1, 1], scaled time, zeros (the same FP32 operations as
+// surrogate.make_inputs).
+__device__ void sc_build_input(const Screen& p, uint8_t* A, int r, int h, uint32_t row) {
+    float x[32];
+    const int c0 = 32 * h;
+    const bool live = row < p.n_rows;
+    const uint32_t cand = live ? row / p.ns : 0u, ti = live ? row % p.ns : 0u;
 #pragma unroll
-    for (int j = 0; j < 64; j++) x[j] = 0.0f;
-    if (row < p.n_rows) {
-        const uint32_t cand = row / p.ns, ti = row % p.ns;
-        for (int j = 0; j < p.n_par; j++) {
+    for (int q = 0; q < 32; q++) {
+        const int j = c0 + q;
+        float v = 0.0f;
+        if (live && j < p.n_par) {
             const float lo = p.log_lo[j], hi = p.log_hi[j];
-            const float v = (2.0f * (p.theta[(size_t)cand * p.n_par + j] - lo)) / (hi - lo) - 1.0f;
-#pragma unroll
-            for (int q = 0; q < 64; q++)
-                if (q == j) x[q] = v;
+            v = (2.0f * (p.theta[(size_t)cand * p.n_par + j] - lo)) / (hi - lo) - 1.0f;
+        } else if (live && j == p.n_par) {
+            v = (2.0f * p.tvec[ti]) / p.t_end - 1.0f;
         }
-        const float tv = (2.0f * p.tvec[ti]) / p.t_end - 1.0f;
-#pragma unroll
-        for (int q = 0; q < 64; q++)
-            if (q == p.n_par) x[q] = tv;
+        x[q] = v;
     }
 #pragma unroll
-    for (int kb = 0; kb < 8; kb++) {
+    for (int kb = 0; kb < 4; kb++) {
         uint4 v;
         v.x = pack_bf2(x[kb * 8 + 0], x[kb * 8 + 1]);
         v.y = pack_bf2(x[kb * 8 + 2], x[kb * 8 + 3]);
         v.z = pack_bf2(x[kb * 8 + 4], x[kb * 8 + 5]);
         v.w = pack_bf2(x[kb * 8 + 6], x[kb * 8 + 7]);
-        *reinterpret_cast<uint4*>(A + canon(r, kb * 8, 128)) = v;
+        *reinterpret_cast<uint4*>(A + canon(r, c0 + kb * 8, 128)) = v;
     }
 }
 
@@ -466,7 +489,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
             mbar_init(&empty[i], 1);
         }
         mbar_init(&acc_full, 1);
-        mbar_init(&a_ready, 128);
+        mbar_init(&a_ready, SC_EPI);
         mbar_init(&drain, 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -482,7 +505,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
 
-    if (warp == 4) {
+    if (warp == 8) {
         // ---- producer: the weight stream, repeated for every tile ----
         if (lane == 0) {
             uint32_t idx = 0;
@@ -510,7 +533,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
                     if (issued[sl]) mbar_wait(&full[sl], (issued[sl] - 1) & 1u, nullptr);
             }
         }
-    } else if (warp == 5) {
+    } else if (warp == 9) {
         // ---- MMA issuer ----
         if (lane == 0) {
             uint32_t idx = 0, nready = 0;
@@ -545,14 +568,16 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
             mbar_wait(&drain, 0u, nullptr);
         }
     } else {
-        // ---- epilogue warps 0-3: thread r owns row r of the tile ----
-        const int r = threadIdx.x;
-        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+        // ---- epilogue warps 0-7: warp w owns rows 32(w%4).. (its TMEM lane
+        // quadrant) and column half w/4; thread r = row of the tile ----
+        const int q = warp & 3, h = warp >> 2;
+        const int r = q * 32 + lane;
+        const uint32_t lane_base = (uint32_t)(q * 32) << 16;
         uint32_t nacc = 0;
         bool ok = true;
         for (uint32_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x) {
             const uint32_t row = t * 128u + (uint32_t)r;
-            sc_build_input(p, A, r, row);
+            sc_build_input(p, A, r, h, row);
             fence_async_smem();
             tc_fence_before();
             mbar_arrive(&a_ready);
@@ -564,27 +589,32 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
                 tc_fence_after();
                 if (l < SC_LAYERS - 1) {
                     const float* b = p.bias + l * SC_HID;
-                    for (int c = 0; c < SC_HID; c += 16) {
-                        float v[16];
-                        tmem_ld16(tmem + lane_base + (uint32_t)c, v);
-                        uint32_t h[8];
+                    for (int c = 128 * h; c < 128 * h + 128; c += 32) {
+                        float v[32];
+                        tmem_ld32(tmem + lane_base + (uint32_t)c, v);
+                        const float4* b4 = reinterpret_cast<const float4*>(b + c);
 #pragma unroll
-                        for (int j = 0; j < 8; j++) {
-                            const float z0 = v[2 * j] + b[c + 2 * j], z1 = v[2 * j + 1] + b[c + 2 * j + 1];
-                            h[j] = pack_bf2(silu(z0), silu(z1));
+                        for (int k = 0; k < 4; k++) {  // 8 columns -> one 16-byte store
+                            const float4 ba = __ldg(b4 + 2 * k), bb = __ldg(b4 + 2 * k + 1);
+                            const float* u = v + 8 * k;
+                            uint4 o;
+                            o.x = pack_bf2(silu(u[0] + ba.x), silu(u[1] + ba.y));
+                            o.y = pack_bf2(silu(u[2] + ba.z), silu(u[3] + ba.w));
+                            o.z = pack_bf2(silu(u[4] + bb.x), silu(u[5] + bb.y));
+                            o.w = pack_bf2(silu(u[6] + bb.z), silu(u[7] + bb.w));
+                            *reinterpret_cast<uint4*>(A + canon(r, c + 8 * k, 128)) = o;
                         }
-                        *reinterpret_cast<uint4*>(A + canon(r, c, 128)) = make_uint4(h[0], h[1], h[2], h[3]);
-                        *reinterpret_cast<uint4*>(A + canon(r, c + 8, 128)) = make_uint4(h[4], h[5], h[6], h[7]);
                     }
                     fence_async_smem();
                     tc_fence_before();
                     mbar_arrive(&a_ready);
                 } else {
-                    // fitness terms of this row: sum_s |target - mean| (/ target when nonzero)
+                    // fitness terms of this row: sum_s |target - mean| (/ target when
+                    // nonzero), 16-column chunks alternating between the two halves
                     const float* b = p.bias + (SC_LAYERS - 1) * SC_HID;
                     float acc = 0.0f;
                     const uint32_t ti = row % p.ns;
-                    for (int c = 0; c < p.S; c += 16) {
+                    for (int c = 16 * h; c < p.S; c += 32) {
                         float v[16];
                         tmem_ld16(tmem + lane_base + (uint32_t)c, v);
 #pragma unroll
@@ -604,9 +634,10 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
                     if (row < p.n_rows) atomicAdd(&s_acc[row / p.ns - cand0], acc);
                     epi_sync();
                     const uint32_t last = (min(t * 128u + 127u, p.n_rows - 1u)) / p.ns;
-                    if ((uint32_t)r <= last - cand0 && t * 128u < p.n_rows) {
-                        atomicAdd(&p.fit[cand0 + r], (double)s_acc[r]);
-                        s_acc[r] = 0.0f;
+                    const int k = threadIdx.x;  // 0..255: one candidate each
+                    if ((uint32_t)k <= last - cand0 && t * 128u < p.n_rows) {
+                        atomicAdd(&p.fit[cand0 + k], (double)s_acc[k]);
+                        s_acc[k] = 0.0f;
                     }
                     epi_sync();
                 }
@@ -751,8 +782,8 @@ extern "C" ctl_status ctl_mlp_screen(const ctl_screen_desc* d, void* stream) {
         set_error("ctl_mlp_screen: need 1 <= n_par <= 63, ns >= 1, 2*S <= out_w <= 256, out_w % 16 == 0, t_end > 0");
         return CTL_ERR_SHAPE;
     }
-    if (reinterpret_cast<uintptr_t>(d->wpack) % 16) {
-        set_error("ctl_mlp_screen: packed weights must be 16-byte aligned");
+    if (reinterpret_cast<uintptr_t>(d->wpack) % 16 || reinterpret_cast<uintptr_t>(d->bias) % 16) {
+        set_error("ctl_mlp_screen: packed weights and biases must be 16-byte aligned");
         return CTL_ERR_ARG;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);

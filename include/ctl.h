@@ -280,7 +280,7 @@ typedef struct {
     int32_t out_w;          /* output layer width (multiple of 16, <= 256) */
     const float* target;    /* [ns][S] */
     const void* wpack;      /* ctl_mlp_pack output (16-byte aligned) */
-    const float* bias;      /* [4*256 + out_w]: the five layers' biases, concatenated */
+    const float* bias;      /* [4*256 + out_w]: the five layers' biases, concatenated (16-byte aligned) */
     double* fitness;        /* [n_cand] out */
     unsigned* err;          /* device word, bit 0 raised if a bounded wait timed out */
 } ctl_screen_desc;
