@@ -95,7 +95,7 @@ struct Run {
 // (consecutive threads hit consecutive banks).  G > 1: slot-contiguous
 // arrays of odd padded length (lanes of one group hit distinct banks).
 struct Layout {
-    uint32_t off_X, off_X1, off_a, off_K, off_tree, off_crit, off_c, off_state, off_list;
+    uint32_t off_X, off_X1, off_a, off_K, off_tree, off_crit, off_c, off_state, off_list, off_grp;
     uint32_t len_S, len_P, len_C, len_T;  // padded lengths (G > 1)
 };
 
@@ -290,36 +290,89 @@ __device__ uint32_t poisson(double lam, uint32_t wa, uint32_t wb, uint64_t seed,
 // Groups and slots
 // ---------------------------------------------------------------------------
 
+// The lanes that work on one simulation.  G <= 32: a slice of one warp
+// (warp-synchronous primitives).  G = 64, 128, 256: whole warps, synchronised
+// by named barrier 1 + group index, cross-warp reductions through a small
+// per-group scratch area in shared memory.
 template <int G>
 struct Grp {
-    uint32_t lane, mask;
+    static constexpr int W = G > 32 ? G / 32 : 1;  // warps per group
+    uint32_t lane, mask, bar;
+    float* fs;                   // [W] per-group scratch (G > 32)
+    unsigned long long* us;      // [W]
+    uint32_t* ws;                // [1]
     __device__ Grp() {
         lane = threadIdx.x % G;
         const uint32_t l = threadIdx.x & 31u;
-        mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (l & ~(uint32_t)(G - 1)));
+        mask = (G >= 32) ? 0xffffffffu : (((1u << G) - 1u) << (l & ~(uint32_t)(G - 1)));
+        bar = 1u + threadIdx.x / G;
+        fs = nullptr;
+        us = nullptr;
+        ws = nullptr;
+    }
+    __device__ __forceinline__ void scratch(unsigned char* base) {  // 16*W + 16 bytes per group
+        unsigned char* b = base + (threadIdx.x / G) * (16 * W + 16);
+        us = reinterpret_cast<unsigned long long*>(b);
+        fs = reinterpret_cast<float*>(b + 8 * W);
+        ws = reinterpret_cast<uint32_t*>(b + 16 * W);
     }
     __device__ __forceinline__ void sync() const {
-        if (G > 1) __syncwarp(mask);
+        if constexpr (G > 32) asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(G) : "memory");
+        else if constexpr (G > 1) __syncwarp(mask);
     }
     __device__ __forceinline__ bool any(bool p) const {
-        if (G == 1) return p;
+        if constexpr (G == 1) return p;
+        if constexpr (G > 32) {
+            uint32_t r;
+            asm volatile(
+                "{\n\t.reg .pred a, b;\n\t"
+                "setp.ne.u32 a, %1, 0;\n\t"
+                "bar.red.or.pred b, %2, %3, a;\n\t"
+                "selp.u32 %0, 1, 0, b;\n\t}"
+                : "=r"(r)
+                : "r"((uint32_t)p), "r"(bar), "r"(G)
+                : "memory");
+            return r != 0;
+        }
         return __any_sync(mask, p) != 0;
     }
     __device__ __forceinline__ float fmin(float v) const {
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) {
+        for (int o = (G < 32 ? G : 32) / 2; o > 0; o >>= 1) {
             float t = __shfl_xor_sync(mask, v, o);
             v = t < v ? t : v;
+        }
+        if constexpr (G > 32) {
+            sync();  // earlier readers of the scratch are done
+            if ((lane & 31u) == 0) fs[lane >> 5] = v;
+            sync();
+            v = fs[0];
+#pragma unroll
+            for (int i = 1; i < W; i++) v = fs[i] < v ? fs[i] : v;
         }
         return v;
     }
     __device__ __forceinline__ unsigned long long sum(unsigned long long v) const {
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+        for (int o = (G < 32 ? G : 32) / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+        if constexpr (G > 32) {
+            sync();
+            if ((lane & 31u) == 0) us[lane >> 5] = v;
+            sync();
+            v = us[0];
+#pragma unroll
+            for (int i = 1; i < W; i++) v += us[i];
+        }
         return v;
     }
     __device__ __forceinline__ uint32_t bcast(uint32_t v) const {
-        if (G == 1) return v;
+        if constexpr (G == 1) return v;
+        if constexpr (G > 32) {
+            sync();
+            if (lane == 0) ws[0] = v;
+            sync();
+            return ws[0];
+        }
         return __shfl_sync(mask, v, 0, G);
     }
 };
@@ -900,6 +953,7 @@ __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layo
     const int NS = (int)(blockDim.x / G);
     const int gi = (int)(threadIdx.x / G);
     Grp<G> g;
+    if constexpr (G > 32) g.scratch(smem + lay.off_grp);
     StateArrays sa;
     {
         unsigned char* b = smem + lay.off_state;
@@ -1260,6 +1314,7 @@ static size_t slot_layout(const HostTables& t, int G, int NS, bool uniform_c, de
     lay.off_c = region(uniform_c ? (size_t)t.P * 4 : (size_t)NS * lay.len_P * 4);
     lay.off_list = region((size_t)NS * 4);
     lay.off_crit = region((size_t)NS * lay.len_C);
+    lay.off_grp = region((size_t)NS * (16 * (G > 32 ? G / 32 : 1) + 16));  // multi-warp group scratch
     return off;
 }
 
@@ -1281,6 +1336,9 @@ static const void* kernel_for(int G, int minb) {
         case 8: return kernel_ptr<8>(minb);
         case 16: return kernel_ptr<16>(minb);
         case 32: return kernel_ptr<32>(minb);
+        case 64: return kernel_ptr<64>(minb);
+        case 128: return kernel_ptr<128>(minb);
+        case 256: return kernel_ptr<256>(minb);
     }
     return nullptr;
 }
@@ -1425,14 +1483,15 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     pl.dec_budget = cfg->dec_budget;
     pl.sched = cfg->sched > 0 ? cfg->sched : 1;
     int G = cfg->group > 0 ? cfg->group : heuristic_group(t);
-    if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32) {
-        set_error("group must be one of 1, 2, 4, 8, 16, 32");
+    if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32 && G != 64 && G != 128 && G != 256) {
+        set_error("group must be a power of two from 1 to 256");
         return CTL_ERR_ARG;
     }
     if (G > t.P) G = t.P;
+    const int tstep = G > 32 ? G : 32;  // blocks hold whole groups and whole warps
     int threads = cfg->threads > 0 ? cfg->threads : 256;
-    if (threads % 32 || threads < 32 || threads > 256) {
-        set_error("threads per block must be a multiple of 32 in [32, 256]");
+    if (threads % tstep || threads < tstep || threads > 256) {
+        set_error("threads per block must be a multiple of 32 and of the group size, at most 256");
         return CTL_ERR_ARG;
     }
     int dev_id = cfg->device;
@@ -1450,7 +1509,7 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     if (ctl_status st = kernel_attr(dev_id, G, minb, ka); st != CTL_OK) return st;
     const size_t smem_max = ka.dyn_max;
     if (cfg->threads <= 0) {
-        while (threads > 32 && (uint64_t)n * G < (uint64_t)threads * da.sm_count) threads -= 32;
+        while (threads > tstep && (uint64_t)n * G < (uint64_t)threads * da.sm_count) threads -= tstep;
     }
     for (;;) {
         int NS = threads / G;
@@ -1460,12 +1519,12 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
             pl.NS = NS;
             break;
         }
-        if (threads <= 32) {
+        if (threads <= tstep) {
             set_error("network too large: one simulation slot needs " + std::to_string(bytes / NS) +
                       " bytes of shared memory");
             return CTL_ERR_SHAPE;
         }
-        threads -= 32;
+        threads -= tstep;
     }
     pl.G = G;
     pl.threads = threads;
@@ -1717,13 +1776,13 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
     int bestG = heuristic_group(t), bestT = 256, bestS = 8, bestD = 2, bestM = 2, bestC = 1;
     float best_ms = 3.4e38f;
     if (e == cudaSuccess) {
-        for (int G = 1; G <= 32 && G <= t.P; G <<= 1) {  // 1. lanes per simulation
+        for (int G = 1; G <= 256 && G <= t.P; G <<= 1) {  // 1. lanes per simulation
             float ms;
             if (time_shape(G, 256, 8, 2, 2, 1, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestG = G; }
         }
         for (int th : {64, 128, 192}) {                   // 2. threads per block
             float ms;
-            if (th % bestG == 0 && time_shape(bestG, th, 8, 2, 2, 1, ms) == CTL_OK && ms < best_ms) {
+            if (th % bestG == 0 && th >= bestG && time_shape(bestG, th, 8, 2, 2, 1, ms) == CTL_OK && ms < best_ms) {
                 best_ms = ms;
                 bestT = th;
             }

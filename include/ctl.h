@@ -85,7 +85,8 @@ typedef struct {
     uint32_t max_steps;   /* per-simulation step cap (CTL_SIM_STEP_LIMIT)              */
     uint32_t sim_base;    /* global index of row 0 (the reference's `offset`)          */
     int32_t device;       /* CUDA device ordinal                                       */
-    int32_t group;        /* lanes per simulation: 1,2,4,8,16,32; 0 = autotune         */
+    int32_t group;        /* lanes per simulation: 1..256, a power of two (above 32: whole
+                             warps per simulation); 0 = library choice                */
     int32_t threads;      /* threads per block; 0 = autotune                           */
     int32_t uniform_rates;/* 1: every row of c equals row 0 (one shared copy per block);
                              ctl_run detects this itself, device calls take it as given */
