@@ -103,3 +103,20 @@ def test_step_limit_status_without_hang():
     assert np.array_equal(out, out_o)
     with pytest.raises(ctl.CtlError):
         m.run(net.X0, net.c, seed=1, max_steps=50)
+
+
+def test_multiwarp_groups_bit_exact():
+    """Groups of 64, 128 and 256 lanes (whole warps per simulation, named
+    barriers and shared-memory reductions) on a 64 x 200 network (256 tree
+    leaves), under both scheduling modes: identical to the oracle."""
+    from cutauleaping_b200 import inputs
+    net = inputs.synthetic(64, 200, 24, seed=13, t_end=0.3, samples=10, x0_range=(10, 5000),
+                           perturb_sigma=0.5, perturb_seed=13)
+    out_o, info_o = oracle_run(net, seed=71)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    for G, threads in ((64, 128), (64, 256), (128, 256), (256, 256)):
+        for sched in (1, 2):
+            out, info = m.run(net.X0, net.c, seed=71, group=G, threads=threads, sched=sched)
+            assert np.array_equal(out, out_o), f"G={G} threads={threads} sched={sched}"
+            assert same_info(info, info_o) is None, f"G={G} threads={threads} sched={sched}"
+            assert m.launch_info(net.n, group=G, threads=threads).group == G
