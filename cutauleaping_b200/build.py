@@ -10,6 +10,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -23,7 +24,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-fmad=false", "-std=c++17",
                      "-Xcompiler", "-fPIC,-ffp-contract=off,-O3", f"-I{INCLUDE}"]
 
-LIB_SOURCES = ["ctl_sweep.cu", "ctl_mlp.cu", "ctl_host.cpp"]
+GROUP_SIZES = (1, 2, 4, 8, 16, 32, 64, 128, 256)
+LIB_SOURCES = (["ctl_sweep.cu", "ctl_mlp.cu", "ctl_host.cpp"] +
+               [f"ctl_sweep_g{g}.cu" for g in GROUP_SIZES])
+OBJ = os.path.join(HERE, "_obj")
 CLI_SOURCES = ["ctl_cli.cpp"]
 
 
@@ -45,7 +49,14 @@ def _run(cmd, verbose):
 def build(force: bool = False, verbose: bool = False) -> None:
     srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
     if force or _newer(LIB, srcs):
-        _run(["nvcc", *NVCC_FLAGS, "-shared", "-o", LIB, *srcs], verbose)
+        # one object per translation unit, compiled in parallel, then linked
+        os.makedirs(OBJ, exist_ok=True)
+        objs = [os.path.join(OBJ, os.path.basename(s) + ".o") for s in srcs]
+        cmds = [["nvcc", *NVCC_FLAGS, "-c", src, "-o", obj] for src, obj in zip(srcs, objs)]
+        jobs = max(1, min(len(cmds), os.cpu_count() or 1))
+        with ThreadPoolExecutor(jobs) as ex:
+            list(ex.map(lambda c: _run(c, verbose), cmds))
+        _run(["nvcc", *ARCH, "-shared", "-o", LIB, *objs], verbose)
     cli_srcs = [os.path.join(CSRC, s) for s in CLI_SOURCES]
     if force or _newer(CLI, cli_srcs + [LIB]):
         _run(["g++", "-O2", "-std=c++17", f"-I{INCLUDE}", "-o", CLI, *cli_srcs,

@@ -1,0 +1,8 @@
+// Sweep kernels for 2 lanes per simulation, in the three register budgets.
+// Each group size has its own translation unit so the build compiles them in
+// parallel.
+#include "ctl_sweep_dev.cuh"
+
+namespace ctl {
+const void* sweep_kernel_g2(int minb) { return dev::sweep_kernel_ptr<2>(minb); }
+}  // namespace ctl
