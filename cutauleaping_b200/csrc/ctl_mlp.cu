@@ -340,22 +340,26 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
 // ---- fused screening: input build -> 5 layers -> fitness, one kernel --------------
 //
 // Screening scores candidates by the surrogate's ensemble mean: rows are
-// (candidate, sample instant) pairs, row = cand * ns + ti.  One CTA owns a
-// 128-row tile at a time (persistent over tiles) and keeps the tile's
-// activations in shared memory for all five layers, so HBM sees only the
-// candidates' parameters and one fitness word per candidate:
-//   * warps 0-3 (epilogue): build the layer-0 input rows, then per layer read
-//     the TMEM accumulator (warp w owns rows 32w..32w+31), add bias, SiLU,
-//     round to BF16 and write the next layer's A operand in place; after the
-//     last layer they accumulate sum_s |target - mean| / target per row and
-//     reduce rows to candidates in shared memory;
-//   * warp 4 (producer): streams the packed weights, 32 K-columns per stage,
-//     with bulk asynchronous copies completing on per-stage mbarriers;
-//   * warp 5 (MMA): one thread issues tcgen05.mma (M = 128, N = layer width,
-//     K = 16) from the activation tile and the weight stage into TMEM.
-// Two CTAs share an SM, so one CTA's epilogue overlaps the other's MMAs.
-constexpr int SC_BK = 32, SC_STAGES = 3, SC_THREADS = 320, SC_EPI = 256, SC_HID = 256, SC_LAYERS = 5;
-constexpr int SC_A_BYTES = 128 * SC_HID * 2;
+// (candidate, sample instant) pairs, row = cand * ns + ti.  One persistent
+// CTA per SM works on two 128-row tiles at a time (ping-pong) and keeps each
+// tile's activations in shared memory for all five layers, so HBM sees only
+// the candidates' parameters and one fitness word per candidate:
+//   * warps 0-7 / 8-15 (epilogue of tile slot 0 / 1): build the layer-0 input
+//     rows, then per layer read the slot's TMEM accumulator (warp w owns rows
+//     32(w%4).. and column half (w/4)%2), add bias, SiLU, round to BF16 and
+//     write the next layer's A operand in place; after the last layer they
+//     accumulate sum_s |target - mean| / target per row and reduce rows to
+//     candidates in shared memory;
+//   * warp 16 (producer): streams the packed weights, 32 K-columns per stage,
+//     6 stages, with bulk asynchronous copies completing on mbarriers;
+//   * warp 17 (MMA): one thread issues tcgen05.mma (M = 128, N = layer width,
+//     K = 16), layer by layer alternating between the two slots, so one
+//     slot's epilogue overlaps the other slot's MMAs.
+// TMEM: 512 columns, 256 per slot.
+constexpr int SC_BK = 32, SC_STAGES = 6, SC_HID = 256, SC_LAYERS = 5;
+constexpr int SC_EPI = 256;                       // epilogue threads per slot
+constexpr int SC_THREADS = 2 * SC_EPI + 64;       // + producer and MMA warps
+constexpr int SC_A_BYTES = 128 * SC_HID * 2;      // one slot's activation tile
 constexpr int SC_STAGE_BYTES = SC_HID * SC_BK * 2;
 
 struct Screen {
@@ -417,18 +421,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
-// Named barrier over the 256 epilogue threads (warps 0-7), and the same
-// barrier as a vote: true when every epilogue thread passes true.
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
-__device__ __forceinline__ bool epi_all(bool v) {
+// Named barrier 1 + slot over one slot's 256 epilogue threads, and the same
+// barrier as a vote: true when every thread of the slot passes true.
+__device__ __forceinline__ void epi_sync(uint32_t id) {
+    asm volatile("bar.sync %0, 256;" ::"r"(id) : "memory");
+}
+__device__ __forceinline__ bool epi_all(uint32_t id, bool v) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred a, b;\n\t"
         "setp.ne.u32 a, %1, 0;\n\t"
-        "bar.red.and.pred b, 1, 256, a;\n\t"
+        "bar.red.and.pred b, %2, 256, a;\n\t"
         "selp.u32 %0, 1, 0, b;\n\t}"
         : "=r"(r)
-        : "r"((uint32_t)v)
+        : "r"((uint32_t)v), "r"(id)
         : "memory");
     return r != 0;
 }
@@ -474,30 +480,38 @@ __device__ void sc_build_input(const Screen& p, uint8_t* A, int r, int h, uint32
     }
 }
 
-__global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
+// Tiles of this CTA: blockIdx.x + i * gridDim.x for i < my_tiles; tile i
+// runs in slot i % 2.
+__device__ __forceinline__ uint32_t sc_my_tiles(const Screen& p) {
+    return blockIdx.x < p.n_tiles ? (p.n_tiles - 1u - blockIdx.x) / gridDim.x + 1u : 0u;
+}
+
+__global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(8) uint64_t full[SC_STAGES], empty[SC_STAGES], acc_full, a_ready, drain;
+    __shared__ __align__(8) uint64_t full[SC_STAGES], empty[SC_STAGES], acc_full[2], a_ready[2], drain;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
-    __shared__ float s_acc[132];
-    uint8_t* A = smem;
-    uint8_t* stage = smem + SC_A_BYTES;
+    __shared__ float s_acc[2][132];
+    uint8_t* stage = smem + 2 * SC_A_BYTES;
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const uint32_t my = sc_my_tiles(p);
     if (threadIdx.x == 0) {
         for (int i = 0; i < SC_STAGES; i++) {
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], 1);
         }
-        mbar_init(&acc_full, 1);
-        mbar_init(&a_ready, SC_EPI);
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&acc_full[i], 1);
+            mbar_init(&a_ready[i], SC_EPI);
+        }
         mbar_init(&drain, 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = threadIdx.x; i < 132; i += SC_THREADS) s_acc[i] = 0.0f;
+    for (int i = threadIdx.x; i < 2 * 132; i += SC_THREADS) (&s_acc[0][0])[i] = 0.0f;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     ::"r"(smem_u32(&tmem_slot)), "r"(SC_HID));
+                     ::"r"(smem_u32(&tmem_slot)), "r"(2 * SC_HID));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -505,25 +519,27 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
 
-    if (warp == 8) {
-        // ---- producer: the weight stream, repeated for every tile ----
+    if (warp == 16) {
+        // ---- producer: the weight stream, in the MMA issuer's order ----
         if (lane == 0) {
             uint32_t idx = 0;
-            uint32_t issued[SC_STAGES] = {0u, 0u, 0u};  // copies issued per slot
+            uint32_t issued[SC_STAGES] = {};  // copies issued per stage buffer
             bool ok = true;
-            for (uint32_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x) {
+            for (uint32_t i0 = 0; i0 < my && ok; i0 += 2) {
                 size_t off = 0;
                 for (int l = 0; l < SC_LAYERS && ok; l++) {
                     const uint32_t bytes = (uint32_t)(sc_n(p, l) * SC_BK * 2);
-                    for (int ks = 0; ks < sc_k(l) / SC_BK; ks++, idx++) {
-                        const uint32_t slot = idx % SC_STAGES, round = idx / SC_STAGES;
-                        if (round > 0 && !mbar_wait(&empty[slot], (round - 1) & 1u, p.err)) { ok = false; break; }
-                        if (*(volatile int*)&abort_flag) { ok = false; break; }
-                        mbar_expect_tx(&full[slot], bytes);
-                        bulk_g2s(stage + slot * SC_STAGE_BYTES, p.wpack + off, bytes, &full[slot]);
-                        issued[slot]++;
-                        off += bytes;
+                    for (uint32_t i = i0; i < i0 + 2 && i < my && ok; i++) {
+                        for (int ks = 0; ks < sc_k(l) / SC_BK; ks++, idx++) {
+                            const uint32_t sl = idx % SC_STAGES, round = idx / SC_STAGES;
+                            if (round > 0 && !mbar_wait(&empty[sl], (round - 1) & 1u, p.err)) { ok = false; break; }
+                            if (*(volatile int*)&abort_flag) { ok = false; break; }
+                            mbar_expect_tx(&full[sl], bytes);
+                            bulk_g2s(stage + sl * SC_STAGE_BYTES, p.wpack + off + (size_t)ks * bytes, bytes, &full[sl]);
+                            issued[sl]++;
+                        }
                     }
+                    off += (size_t)bytes * (sc_k(l) / SC_BK);
                 }
             }
             if (!ok) {
@@ -533,34 +549,42 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
                     if (issued[sl]) mbar_wait(&full[sl], (issued[sl] - 1) & 1u, nullptr);
             }
         }
-    } else if (warp == 9) {
-        // ---- MMA issuer ----
+    } else if (warp == 17) {
+        // ---- MMA issuer: per tile pair and layer, slot 0 then slot 1 ----
         if (lane == 0) {
-            uint32_t idx = 0, nready = 0;
+            uint32_t idx = 0, nready[2] = {0u, 0u};
             bool ok = true;
-            const uint32_t a0 = smem_u32(A), s0 = smem_u32(stage);
-            for (uint32_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x) {
+            const uint32_t s0 = smem_u32(stage);
+            for (uint32_t i0 = 0; i0 < my && ok; i0 += 2) {
                 for (int l = 0; l < SC_LAYERS && ok; l++) {
-                    if (!mbar_wait(&a_ready, nready & 1u, p.err) || *(volatile int*)&abort_flag) { ok = false; break; }
-                    nready++;
-                    tc_fence_after();
                     const int N = sc_n(p, l);
                     const uint32_t idesc = make_idesc(128, N);
-                    for (int ks = 0; ks < sc_k(l) / SC_BK; ks++, idx++) {
-                        const uint32_t slot = idx % SC_STAGES, round = idx / SC_STAGES;
-                        if (!mbar_wait(&full[slot], round & 1u, p.err)) { ok = false; break; }
-                        tc_fence_after();
-#pragma unroll
-                        for (int kk = 0; kk < SC_BK / 16; kk++) {
-                            const int k0 = ks * SC_BK + kk * 16;  // K offset in the activation tile
-                            const uint64_t da = make_desc(a0 + (uint32_t)(k0 / 8) * 16u * 128u, 16u * 128u, 128u);
-                            const uint64_t db = make_desc(s0 + slot * SC_STAGE_BYTES + (uint32_t)(kk * 2 * (N / 8) * 128),
-                                                          (uint32_t)((N / 8) * 128), 128u);
-                            mma_bf16(tmem, da, db, idesc, (ks > 0 || kk > 0) ? 1u : 0u);
+                    for (uint32_t i = i0; i < i0 + 2 && i < my && ok; i++) {
+                        const uint32_t slot = i & 1u;
+                        if (!mbar_wait(&a_ready[slot], nready[slot] & 1u, p.err) || *(volatile int*)&abort_flag) {
+                            ok = false;
+                            break;
                         }
-                        mma_commit(&empty[slot]);
+                        nready[slot]++;
+                        tc_fence_after();
+                        const uint32_t a0 = smem_u32(smem + slot * SC_A_BYTES);
+                        const uint32_t d = tmem + slot * SC_HID;
+                        for (int ks = 0; ks < sc_k(l) / SC_BK; ks++, idx++) {
+                            const uint32_t sl = idx % SC_STAGES, round = idx / SC_STAGES;
+                            if (!mbar_wait(&full[sl], round & 1u, p.err)) { ok = false; break; }
+                            tc_fence_after();
+#pragma unroll
+                            for (int kk = 0; kk < SC_BK / 16; kk++) {
+                                const int k0 = ks * SC_BK + kk * 16;  // K offset in the activation tile
+                                const uint64_t da = make_desc(a0 + (uint32_t)(k0 / 8) * 16u * 128u, 16u * 128u, 128u);
+                                const uint64_t db = make_desc(s0 + sl * SC_STAGE_BYTES + (uint32_t)(kk * 2 * (N / 8) * 128),
+                                                              (uint32_t)((N / 8) * 128), 128u);
+                                mma_bf16(d, da, db, idesc, (ks > 0 || kk > 0) ? 1u : 0u);
+                            }
+                            mma_commit(&empty[sl]);
+                        }
+                        if (ok) mma_commit(&acc_full[slot]);
                     }
-                    if (ok) mma_commit(&acc_full);
                 }
             }
             if (!ok) atomicExch(&abort_flag, 1);
@@ -568,22 +592,28 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
             mbar_wait(&drain, 0u, nullptr);
         }
     } else {
-        // ---- epilogue warps 0-7: warp w owns rows 32(w%4).. (its TMEM lane
-        // quadrant) and column half w/4; thread r = row of the tile ----
-        const int q = warp & 3, h = warp >> 2;
+        // ---- epilogue of slot e = warp / 8: warp w owns rows 32(w%4).. (its
+        // TMEM lane quadrant) and column half (w/4)%2; thread r = row ----
+        const uint32_t e = (uint32_t)warp >> 3;
+        const uint32_t bar_id = 1u + e;
+        const int q = warp & 3, h = (warp >> 2) & 1;
         const int r = q * 32 + lane;
-        const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+        const int et = (int)threadIdx.x - (int)e * SC_EPI;  // 0..255 within the slot
+        uint8_t* A = smem + e * SC_A_BYTES;
+        float* acc_c = s_acc[e];
+        const uint32_t tbase = tmem + e * SC_HID + ((uint32_t)(q * 32) << 16);
         uint32_t nacc = 0;
         bool ok = true;
-        for (uint32_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x) {
+        for (uint32_t i = e; i < my && ok; i += 2) {
+            const uint32_t t = blockIdx.x + i * gridDim.x;
             const uint32_t row = t * 128u + (uint32_t)r;
             sc_build_input(p, A, r, h, row);
             fence_async_smem();
             tc_fence_before();
-            mbar_arrive(&a_ready);
+            mbar_arrive(&a_ready[e]);
             for (int l = 0; l < SC_LAYERS; l++) {
-                bool got = mbar_wait(&acc_full, nacc & 1u, p.err);
-                got = epi_all(got && !*(volatile int*)&abort_flag);  // uniform: the epilogue holds named barriers
+                bool got = mbar_wait(&acc_full[e], nacc & 1u, p.err);
+                got = epi_all(bar_id, got && !*(volatile int*)&abort_flag);  // uniform over the slot
                 nacc++;
                 if (!got) { ok = false; break; }
                 tc_fence_after();
@@ -591,7 +621,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
                     const float* b = p.bias + l * SC_HID;
                     for (int c = 128 * h; c < 128 * h + 128; c += 32) {
                         float v[32];
-                        tmem_ld32(tmem + lane_base + (uint32_t)c, v);
+                        tmem_ld32(tbase + (uint32_t)c, v);
                         const float4* b4 = reinterpret_cast<const float4*>(b + c);
 #pragma unroll
                         for (int k = 0; k < 4; k++) {  // 8 columns -> one 16-byte store
@@ -607,7 +637,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
                     }
                     fence_async_smem();
                     tc_fence_before();
-                    mbar_arrive(&a_ready);
+                    mbar_arrive(&a_ready[e]);
                 } else {
                     // fitness terms of this row: sum_s |target - mean| (/ target when
                     // nonzero), 16-column chunks alternating between the two halves
@@ -616,7 +646,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
                     const uint32_t ti = row % p.ns;
                     for (int c = 16 * h; c < p.S; c += 32) {
                         float v[16];
-                        tmem_ld16(tmem + lane_base + (uint32_t)c, v);
+                        tmem_ld16(tbase + (uint32_t)c, v);
 #pragma unroll
                         for (int j = 0; j < 16; j++) {
                             const int s_ = c + j;
@@ -631,15 +661,14 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
                     }
                     tc_fence_before();
                     const uint32_t cand0 = (t * 128u) / p.ns;
-                    if (row < p.n_rows) atomicAdd(&s_acc[row / p.ns - cand0], acc);
-                    epi_sync();
+                    if (row < p.n_rows) atomicAdd(&acc_c[row / p.ns - cand0], acc);
+                    epi_sync(bar_id);
                     const uint32_t last = (min(t * 128u + 127u, p.n_rows - 1u)) / p.ns;
-                    const int k = threadIdx.x;  // 0..255: one candidate each
-                    if ((uint32_t)k <= last - cand0 && t * 128u < p.n_rows) {
-                        atomicAdd(&p.fit[cand0 + k], (double)s_acc[k]);
-                        s_acc[k] = 0.0f;
+                    if ((uint32_t)et <= last - cand0 && t * 128u < p.n_rows) {
+                        atomicAdd(&p.fit[cand0 + et], (double)acc_c[et]);
+                        acc_c[et] = 0.0f;
                     }
-                    epi_sync();
+                    epi_sync(bar_id);
                 }
             }
         }
@@ -647,7 +676,8 @@ __global__ void __launch_bounds__(SC_THREADS, 2) screen_kernel(Screen p) {
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(SC_HID));
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * SC_HID));
 }
 
 // Packs a BF16 weight matrix W [N][K] (K contiguous, row stride ldw) into
@@ -800,7 +830,7 @@ extern "C" ctl_status ctl_mlp_screen(const ctl_screen_desc* d, void* stream) {
     p.tvec = d->tvec; p.t_end = d->t_end; p.log_lo = d->log_lo; p.log_hi = d->log_hi;
     p.y_mean = d->y_mean; p.y_std = d->y_std; p.S = d->S; p.out_w = d->out_w; p.target = d->target;
     p.wpack = static_cast<const uint8_t*>(d->wpack); p.bias = d->bias; p.fit = d->fitness; p.err = d->err;
-    const size_t smem = (size_t)mlp::SC_A_BYTES + (size_t)mlp::SC_STAGES * mlp::SC_STAGE_BYTES;
+    const size_t smem = (size_t)2 * mlp::SC_A_BYTES + (size_t)mlp::SC_STAGES * mlp::SC_STAGE_BYTES;
     static int sms[16];
     int dev = 0;
     if ((st = mlp_cuda(cudaGetDevice(&dev), "cudaGetDevice")) != CTL_OK) return st;
@@ -814,7 +844,7 @@ extern "C" ctl_status ctl_mlp_screen(const ctl_screen_desc* d, void* stream) {
             return st;
         sms[dev] = n;
     }
-    const uint32_t grid = std::min<uint32_t>(p.n_tiles, 2u * (uint32_t)sms[dev]);
+    const uint32_t grid = std::min<uint32_t>(p.n_tiles, (uint32_t)sms[dev]);  // one CTA per SM
     mlp::screen_kernel<<<grid, mlp::SC_THREADS, smem, s>>>(p);
     if ((st = mlp_cuda(cudaGetLastError(), "screen_kernel launch")) != CTL_OK) return st;
     mlp::scale_kernel<<<(d->n_cand + 255) / 256, 256, 0, s>>>(d->fitness, d->n_cand,
