@@ -211,6 +211,26 @@ def screen_roofline(p, net, sc, n_cand):
             "peak_source": "MEASURED_PEAKS.json bf16_tflops (measured, burst)"}
 
 
+def bench_screen(a):
+    """The fused screening kernel alone (config 5's tensor-core part): a
+    briefly trained surrogate of the config-5 network scores 200,000
+    candidates x 50 instants per launch; prints its roofline line."""
+    import torch
+    from cutauleaping_b200 import fitsearch as fs
+    p = fs.make_problem(n_rep=8, samples=50, t_end=5.0)
+    theta, traj = fs.training_data(p, 1 << 14)
+    net, sc = fs.train_surrogate(p, theta, traj, epochs=1, batch=8192)
+    torch.cuda.synchronize()
+    r = screen_roofline(p, net, sc, n_cand=200_000)
+    net.check_error_flag()
+    print(json.dumps({"metric": "screened candidate-instants/s (fused surrogate screening kernel)",
+                      "value": r["rows_per_launch"] / (r["launch_ms"] * 1e-3), "unit": "rows/s",
+                      "higher_is_better": True, "n_gpus": 1, "dtype": "bf16 (fp32 accumulate)",
+                      "data": "synthetic", "config": {"workload": "screening of 200,000 candidates x 50 instants, "
+                                                                  "9 -> 256 x 4 -> 64 MLP + fitness"},
+                      "roofline": r, "gpu_launches": 10}), flush=True)
+
+
 def bench_config5(a):
     """Surrogate-screened parameter estimation against plain-simulator search.
 
@@ -284,13 +304,14 @@ def main():
     ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5])
     ap.add_argument("--full", action="store_true", help="config 5 at the configured sizes")
     ap.add_argument("--inner", type=int, default=1, help="config 5: surrogate-only iterations per generation")
+    ap.add_argument("--screen-only", action="store_true", help="config 5: time the fused screening kernel alone")
     ap.add_argument("--finetune", type=int, default=100,
                     help="config 5: surrogate fine-tuning steps per generation on the re-simulated trajectories")
     ap.add_argument("--sims", type=int, default=None, help="simulations per GPU (default: config's)")
     ap.add_argument("--group", type=int, default=0, help="lanes per simulation (0 = library choice)")
     ap.add_argument("--threads", type=int, default=0, help="threads per block (0 = library choice)")
     ap.add_argument("--min-blocks", type=int, default=0,
-                    help="register budget of the sweep kernel: 1, 3 or 4 resident blocks (0 = library choice)")
+                    help="register budget of the sweep kernel: 2, 3 or 4 resident blocks (0 = library choice)")
     ap.add_argument("--sched", type=int, default=0,
                     help="scheduling: 1 block regrouping rounds, 2 warp-local (0 = library choice)")
     ap.add_argument("--autotune", action="store_true", help="measure launch shapes before timing")
@@ -301,6 +322,10 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if a.config == 5 and a.screen_only:
+        if rank == 0 and a.impl == "ours":
+            bench_screen(a)
+        return
     if a.config == 5:
         if rank == 0 and a.impl == "ours":
             bench_config5(a)
