@@ -164,13 +164,21 @@ int main(int argc, const char* argv[]) {
         fprintf(stdout, " * 3P-tau-leaping starting on GPU%d\n", gpu);
     }
 
-    std::vector<uint32_t> samples((size_t)N * dims.ns * dims.s_out);
     std::vector<ctl_sim_info> info(N);
+    std::vector<uint32_t> samples;
+    std::vector<double> fit;
     struct timespec t0, t1;
     clock_gettime(CLOCK_MONOTONIC, &t0);
-    st = ctl_run(model, &cfg, N, X0.data(), c.data(), samples.data(), info.data());
+    if (just_fitness) {
+        // fitness mode: samples are summed per parameter set on the device
+        fit.assign(N, 0.0);
+        st = ctl_fitness_run(model, target, &cfg, X0.data(), c.data(), fit.data(), info.data());
+    } else {
+        samples.resize((size_t)N * dims.ns * dims.s_out);
+        st = ctl_run(model, &cfg, N, X0.data(), c.data(), samples.data(), info.data());
+    }
     clock_gettime(CLOCK_MONOTONIC, &t1);
-    if (st != CTL_OK && st != CTL_ERR_STEP_LIMIT) return exit_code(st, "run");
+    if (st != CTL_OK && st != CTL_ERR_STEP_LIMIT) return exit_code(st, just_fitness ? "fitness" : "run");
     if (st == CTL_ERR_STEP_LIMIT) fprintf(stderr, "WARNING: %s\n", ctl_last_error());
     if (verbose)
         printf(" * RUNNING TIME: %f seconds.\n", (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec));
@@ -188,9 +196,6 @@ int main(int argc, const char* argv[]) {
         if (st != CTL_OK) return exit_code(st, "output");
     } else {
         if (verbose) printf(" * Calculating fitnesses.\n");
-        std::vector<double> fit(N, 0.0);
-        st = ctl_fitness(model, target, &cfg, samples.data(), fit.data());
-        if (st != CTL_OK) return exit_code(st, "fitness");
         uint32_t prep = 1;
         ctl_target_dims(target, nullptr, &prep, nullptr, nullptr);
         fflush(stdout);

@@ -351,16 +351,17 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
 //     accumulate sum_s |target - mean| / target per row and reduce rows to
 //     candidates in shared memory;
 //   * warp 16 (producer): streams the packed weights, 32 K-columns per stage,
-//     6 stages, with bulk asynchronous copies completing on mbarriers;
+//     5 stages, with bulk asynchronous copies completing on mbarriers;
 //   * warp 17 (MMA): one thread issues tcgen05.mma (M = 128, N = layer width,
 //     K = 16), layer by layer alternating between the two slots, so one
 //     slot's epilogue overlaps the other slot's MMAs.
 // TMEM: 512 columns, 256 per slot.
-constexpr int SC_BK = 32, SC_STAGES = 6, SC_HID = 256, SC_LAYERS = 5;
+constexpr int SC_BK = 32, SC_STAGES = 5, SC_HID = 256, SC_LAYERS = 5;
 constexpr int SC_EPI = 256;                       // epilogue threads per slot
 constexpr int SC_THREADS = 2 * SC_EPI + 64;       // + producer and MMA warps
 constexpr int SC_A_BYTES = 128 * SC_HID * 2;      // one slot's activation tile
 constexpr int SC_STAGE_BYTES = SC_HID * SC_BK * 2;
+constexpr int SC_CONST_BYTES = 16384;             // biases, output scaling, target (when it fits)
 
 struct Screen {
     const float* theta;   // [n_cand][n_par]
@@ -444,9 +445,10 @@ __device__ __forceinline__ uint32_t canon(int row, int k, int rows) {
     return (uint32_t)(((k >> 3) * (rows >> 3) + (row >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
+// Two FP32 values -> two BF16 (round to nearest even) in one conversion.
 __device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
-    const __nv_bfloat16 x = __float2bfloat16(a), y = __float2bfloat16(b);
-    return (uint32_t)__bfloat16_as_ushort(x) | ((uint32_t)__bfloat16_as_ushort(y) << 16);
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&v);
 }
 
 // Layer-0 input columns [32h, 32h + 32) of row r of the tile: scaled log
@@ -493,6 +495,21 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
     __shared__ int abort_flag;
     __shared__ float s_acc[2][132];
     uint8_t* stage = smem + 2 * SC_A_BYTES;
+    // per-CTA constants in shared memory: biases [4*256 + out_w], y_mean [S],
+    // y_std [S], and the target [ns][S] when it fits
+    float* c_bias = reinterpret_cast<float*>(stage + SC_STAGES * SC_STAGE_BYTES);
+    float* c_ym = c_bias + 4 * SC_HID + p.out_w;
+    float* c_ys = c_ym + p.S;
+    float* c_tg = c_ys + p.S;
+    const bool tg_smem = (size_t)(4 * SC_HID + p.out_w + 2 * p.S + p.ns * p.S) * 4 <= (size_t)SC_CONST_BYTES;
+    const float* tgt = tg_smem ? c_tg : p.target;
+    for (int i = threadIdx.x; i < 4 * SC_HID + p.out_w; i += SC_THREADS) c_bias[i] = p.bias[i];
+    for (int i = threadIdx.x; i < p.S; i += SC_THREADS) {
+        c_ym[i] = p.y_mean[i];
+        c_ys[i] = p.y_std[i];
+    }
+    if (tg_smem)
+        for (int i = threadIdx.x; i < (int)(p.ns * p.S); i += SC_THREADS) c_tg[i] = p.target[i];
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const uint32_t my = sc_my_tiles(p);
     if (threadIdx.x == 0) {
@@ -618,14 +635,14 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
                 if (!got) { ok = false; break; }
                 tc_fence_after();
                 if (l < SC_LAYERS - 1) {
-                    const float* b = p.bias + l * SC_HID;
+                    const float* b = c_bias + l * SC_HID;
                     for (int c = 128 * h; c < 128 * h + 128; c += 32) {
                         float v[32];
                         tmem_ld32(tbase + (uint32_t)c, v);
                         const float4* b4 = reinterpret_cast<const float4*>(b + c);
 #pragma unroll
                         for (int k = 0; k < 4; k++) {  // 8 columns -> one 16-byte store
-                            const float4 ba = __ldg(b4 + 2 * k), bb = __ldg(b4 + 2 * k + 1);
+                            const float4 ba = b4[2 * k], bb = b4[2 * k + 1];
                             const float* u = v + 8 * k;
                             uint4 o;
                             o.x = pack_bf2(silu(u[0] + ba.x), silu(u[1] + ba.y));
@@ -641,7 +658,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
                 } else {
                     // fitness terms of this row: sum_s |target - mean| (/ target when
                     // nonzero), 16-column chunks alternating between the two halves
-                    const float* b = p.bias + (SC_LAYERS - 1) * SC_HID;
+                    const float* b = c_bias + (SC_LAYERS - 1) * SC_HID;
                     float acc = 0.0f;
                     const uint32_t ti = row % p.ns;
                     for (int c = 16 * h; c < p.S; c += 32) {
@@ -651,8 +668,8 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
                         for (int j = 0; j < 16; j++) {
                             const int s_ = c + j;
                             if (s_ < p.S && row < p.n_rows) {
-                                const float mean = (v[j] + b[s_]) * p.y_std[s_] + p.y_mean[s_];
-                                const float tg = p.target[(size_t)ti * p.S + s_];
+                                const float mean = (v[j] + b[s_]) * c_ys[s_] + c_ym[s_];
+                                const float tg = tgt[(size_t)ti * p.S + s_];
                                 float d = fabsf(tg - mean);
                                 if (tg != 0.0f) d = d / tg;
                                 acc += d;
@@ -830,7 +847,8 @@ extern "C" ctl_status ctl_mlp_screen(const ctl_screen_desc* d, void* stream) {
     p.tvec = d->tvec; p.t_end = d->t_end; p.log_lo = d->log_lo; p.log_hi = d->log_hi;
     p.y_mean = d->y_mean; p.y_std = d->y_std; p.S = d->S; p.out_w = d->out_w; p.target = d->target;
     p.wpack = static_cast<const uint8_t*>(d->wpack); p.bias = d->bias; p.fit = d->fitness; p.err = d->err;
-    const size_t smem = (size_t)2 * mlp::SC_A_BYTES + (size_t)mlp::SC_STAGES * mlp::SC_STAGE_BYTES;
+    const size_t smem = (size_t)2 * mlp::SC_A_BYTES + (size_t)mlp::SC_STAGES * mlp::SC_STAGE_BYTES +
+                        (size_t)mlp::SC_CONST_BYTES;
     static int sms[16];
     int dev = 0;
     if ((st = mlp_cuda(cudaGetDevice(&dev), "cudaGetDevice")) != CTL_OK) return st;

@@ -66,6 +66,31 @@ __global__ void fitness_kernel(const uint32_t* __restrict__ samples, const uint3
     fitness[tid] = ((1.0 / (double)ns) * (1.0 / (double)so)) * (double)sub;
 }
 
+// The same from per-set sample sums (fitness mode of the sweep): the
+// reference's FP64 running sum of p_rep integer samples is exact, so it
+// equals the integer sum converted once; the rest is calculateFitness.
+__global__ void fitness_sums_kernel(const unsigned long long* __restrict__ sums, const uint32_t* __restrict__ target,
+                                    const uint8_t* __restrict__ swarm, double* __restrict__ fitness,
+                                    uint32_t nsets, uint32_t p_rep, uint32_t ns, uint32_t so, uint32_t E,
+                                    uint32_t REP) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= nsets) return;
+    const uint32_t ex = swarm[tid];
+    float sub = 0.0f;
+    for (uint32_t c = 0; c < ns; c++) {
+        for (uint32_t s = 0; s < so; s++) {
+            const double acc = (double)sums[((size_t)tid * ns + c) * so + s] / (double)p_rep;
+            for (uint32_t e = 0; e < REP; e++) {
+                const int tgt = (int)target[((size_t)(c * E + ex) * REP + e) * so + s];
+                double dist = fabs((double)tgt - acc);
+                if (tgt != 0) dist = dist / (double)tgt;
+                sub = (float)((double)sub + dist);
+            }
+        }
+    }
+    fitness[tid] = ((1.0 / (double)ns) * (1.0 / (double)so)) * (double)sub;
+}
+
 }  // namespace dev
 
 // ---------------------------------------------------------------------------
@@ -225,7 +250,7 @@ static int tree_words(const HostTables& t) {
 }
 
 // Shared-memory bytes of a block with NS slots of group size G.
-static size_t slot_layout(const HostTables& t, int G, int NS, bool uniform_c, dev::Layout& lay) {
+static size_t slot_layout(const HostTables& t, int G, int NS, bool uniform_c, dev::Layout& lay, bool sums = false) {
     size_t off = 0;
     auto region = [&](size_t bytes) {
         size_t o = off;
@@ -238,11 +263,13 @@ static size_t slot_layout(const HostTables& t, int G, int NS, bool uniform_c, de
         lay.len_P = (uint32_t)t.P;
         lay.len_C = (uint32_t)t.P;
         lay.len_T = (uint32_t)tw;
+        lay.len_O = (uint32_t)t.s_out;
     } else {
         lay.len_S = (uint32_t)(t.S | 1);
         lay.len_P = (uint32_t)(t.P + 1);
         lay.len_C = (uint32_t)(((t.P + 3) & ~3) + 4);
         lay.len_T = (uint32_t)(tw | 1);
+        lay.len_O = (uint32_t)(t.s_out | 1);
     }
     lay.off_tree = region((size_t)NS * lay.len_T * 8);
     lay.off_state = region((size_t)NS * (4 * 8 + 9 * 4));
@@ -254,6 +281,7 @@ static size_t slot_layout(const HostTables& t, int G, int NS, bool uniform_c, de
     lay.off_list = region((size_t)NS * 4);
     lay.off_crit = region((size_t)NS * lay.len_C);
     lay.off_grp = region((size_t)NS * (16 * (G > 32 ? G / 32 : 1) + 16));  // multi-warp group scratch
+    lay.off_last = region(sums ? (size_t)NS * lay.len_O * 4 : 0);         // fitness mode only
     return off;
 }
 
@@ -393,7 +421,8 @@ static bool find_tuned(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, ctl_mod
     return false;
 }
 
-static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t n, LaunchPlan& pl) {
+static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t n, LaunchPlan& pl,
+                              bool sums = false) {
     const HostTables& t = m->t;
     ctl_run_cfg tuned_cfg = *cfg_in;
     if (cfg_in->group <= 0 && cfg_in->threads <= 0) {
@@ -432,7 +461,7 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     // 256-thread block allows (2 or 3; 4 only when chosen or tuned).
     int minb = cfg->min_blocks;
     if (minb <= 0) {
-        const size_t full = slot_layout(t, G, 256 / G, uni, pl.lay);
+        const size_t full = slot_layout(t, G, 256 / G, uni, pl.lay, sums);
         minb = 3 * (full + 1024) <= (size_t)da.smem_optin + 1024 ? 3 : 2;
     }
     if (ctl_status st = kernel_attr(dev_id, G, minb, ka); st != CTL_OK) return st;
@@ -442,7 +471,7 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     }
     for (;;) {
         int NS = threads / G;
-        size_t bytes = slot_layout(t, G, NS, uni, pl.lay);
+        size_t bytes = slot_layout(t, G, NS, uni, pl.lay, sums);
         if (bytes <= smem_max) {
             pl.smem = bytes;
             pl.NS = NS;
@@ -475,7 +504,9 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
 
 static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* dX0,
                                 const float* dc, uint32_t* dout, ctl_sim_info* dinfo,
-                                cudaStream_t stream, const LaunchPlan& pl, const DeviceCopy& d) {
+                                cudaStream_t stream, const LaunchPlan& pl, const DeviceCopy& d,
+                                unsigned long long* sums = nullptr, uint32_t sum_threads = 1,
+                                uint32_t sum_prep = 1) {
     dev::Run run;
     run.seed = cfg->seed;
     run.eps = cfg->eps;
@@ -493,6 +524,9 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.X0 = dX0;
     run.c = dc;
     run.out = dout;
+    run.sums = sums;
+    run.sum_threads = sum_threads;
+    run.sum_prep = sum_prep;
     run.info = dinfo;
     run.queue = d.ctrl;
     dev::Model dm = make_dev_model(m, d, cfg->flags);
@@ -873,6 +907,135 @@ extern "C" ctl_status ctl_fitness(ctl_model* m, const ctl_target* t, const ctl_r
     cudaStreamDestroy(s);
     if (e != cudaSuccess) return cuda_fail(e, "ctl_fitness");
     if (e2 != cudaSuccess) return cuda_fail(e2, "ctl_fitness (kernel)");
+    return CTL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Fitness mode without per-simulation samples
+// ---------------------------------------------------------------------------
+
+static ctl_status check_sums_shape(uint32_t n, uint32_t threads, uint32_t p_rep) {
+    if (!threads || !p_rep || n % threads || (n / threads) % p_rep) {
+        set_error("fitness mode needs n = threads * blocks with blocks a multiple of p_rep");
+        return CTL_ERR_ARG;
+    }
+    return CTL_OK;
+}
+
+extern "C" ctl_status ctl_run_device_sums(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* d_X0,
+                                          const float* d_c, uint32_t threads, uint32_t p_rep, uint64_t* d_sums,
+                                          ctl_sim_info* d_info, void* stream) {
+    if (!m) return CTL_ERR_ARG;
+    ctl_status st = check_cfg(cfg);
+    if (st != CTL_OK) return st;
+    if (n == 0) return CTL_OK;
+    if ((st = check_sums_shape(n, threads, p_rep)) != CTL_OK) return st;
+    if (!d_X0 || !d_c || !d_sums || !d_info) {
+        set_error("null device buffer");
+        return CTL_ERR_ARG;
+    }
+    DeviceGuard dg(cfg->device);
+    DeviceCopy* d = nullptr;
+    if ((st = ensure_device(m, cfg->device, d)) != CTL_OK) return st;
+    LaunchPlan pl;
+    if ((st = plan_launch(m, cfg, n, pl, true)) != CTL_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t words = (size_t)(n / p_rep) * m->t.ns * m->t.s_out;
+    CTL_CUDA(cudaMemsetAsync(d_sums, 0, words * 8, s));
+    return enqueue_sweep(m, cfg, n, d_X0, d_c, nullptr, d_info, s, pl, *d,
+                         reinterpret_cast<unsigned long long*>(d_sums), threads, p_rep);
+}
+
+extern "C" ctl_status ctl_fitness_sums_device(const uint64_t* d_sums, uint32_t ns, uint32_t s_out,
+                                              const uint32_t* d_target, const uint8_t* d_experiment,
+                                              uint32_t experiments, uint32_t repetitions, uint32_t threads,
+                                              uint32_t blocks, uint32_t p_rep, double* d_fitness, void* stream) {
+    if (!d_sums || !d_target || !d_experiment || !d_fitness || !threads || !blocks || !p_rep ||
+        blocks % p_rep || !ns || !s_out) {
+        set_error("ctl_fitness_sums_device: invalid argument");
+        return CTL_ERR_ARG;
+    }
+    const uint32_t nsets = (uint32_t)(((uint64_t)threads * blocks) / p_rep);
+    dev::fitness_sums_kernel<<<(nsets + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const unsigned long long*>(d_sums), d_target, d_experiment, d_fitness, nsets, p_rep, ns,
+        s_out, experiments, repetitions);
+    CTL_CUDA(cudaGetLastError());
+    return CTL_OK;
+}
+
+extern "C" ctl_status ctl_fitness_run(ctl_model* m, const ctl_target* t, const ctl_run_cfg* cfg, const int32_t* X0,
+                                      const float* c, double* fitness, ctl_sim_info* info) {
+    if (!m || !t || !X0 || !c || !fitness || !info) return CTL_ERR_ARG;
+    ctl_status st = check_cfg(cfg);
+    if (st != CTL_OK) return st;
+    const HostTables& h = m->t;
+    if (t->ns != (uint32_t)h.ns || t->s_out != (uint32_t)h.s_out) {
+        set_error("fitness target does not match the model's samples");
+        return CTL_ERR_SHAPE;
+    }
+    const uint64_t N64 = (uint64_t)t->threads * t->blocks;
+    if (N64 == 0 || N64 > 0xffffffffull) return CTL_ERR_ARG;
+    const uint32_t N = (uint32_t)N64;
+    if ((st = check_sums_shape(N, t->threads, t->p_rep)) != CTL_OK) return st;
+    const uint32_t nsets = N / t->p_rep;
+    DeviceGuard dg(cfg->device);
+    DeviceCopy* d = nullptr;
+    if ((st = ensure_device(m, cfg->device, d)) != CTL_OK) return st;
+    ctl_run_cfg rc = *cfg;
+    if (!rc.uniform_rates) {
+        bool same = true;
+        for (uint32_t i = 1; i < N && same; i++)
+            same = std::memcmp(c + (size_t)i * h.R, c, (size_t)h.R * sizeof(float)) == 0;
+        rc.uniform_rates = same ? 1 : 0;
+    }
+    LaunchPlan pl;
+    if ((st = plan_launch(m, &rc, N, pl, true)) != CTL_OK) return st;
+    keep_pool_memory(cfg->device);
+    const size_t bx = (size_t)N * h.S * 4, bc = (size_t)N * h.R * 4, bi = (size_t)N * sizeof(ctl_sim_info);
+    const size_t bsum = (size_t)nsets * h.ns * h.s_out * 8, bt = t->series.size() * 4, bw = (size_t)N;
+    cudaStream_t s;
+    CTL_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    void *dx = nullptr, *dc = nullptr, *dinf = nullptr, *dsum = nullptr, *dt = nullptr, *dw = nullptr, *df = nullptr;
+    cudaError_t e = cudaMallocAsync(&dx, bx, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dc, bc, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dinf, bi, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dsum, bsum, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dt, std::max<size_t>(bt, 4), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dw, std::max<size_t>(bw, 4), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&df, (size_t)N * 8, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dx, X0, bx, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dc, c, bc, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && bt) e = cudaMemcpyAsync(dt, t->series.data(), bt, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dw, t->thread2experiment.data(), bw, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dsum, 0, bsum, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(df, 0, (size_t)N * 8, s);
+    if (e == cudaSuccess) {
+        st = enqueue_sweep(m, &rc, N, static_cast<int32_t*>(dx), static_cast<float*>(dc), nullptr,
+                           static_cast<ctl_sim_info*>(dinf), s, pl, *d, static_cast<unsigned long long*>(dsum),
+                           t->threads, t->p_rep);
+        if (st != CTL_OK) e = cudaErrorLaunchFailure;
+    }
+    if (e == cudaSuccess && nsets) {
+        dev::fitness_sums_kernel<<<(nsets + 127) / 128, 128, 0, s>>>(
+            static_cast<unsigned long long*>(dsum), static_cast<uint32_t*>(dt), static_cast<uint8_t*>(dw),
+            static_cast<double*>(df), nsets, t->p_rep, (uint32_t)h.ns, (uint32_t)h.s_out, t->experiments,
+            t->repetitions);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(fitness, df, (size_t)N * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(info, dinf, bi, cudaMemcpyDeviceToHost, s);
+    for (void* p : {dx, dc, dinf, dsum, dt, dw, df})
+        if (p) cudaFreeAsync(p, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (st != CTL_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "ctl_fitness_run");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "ctl_fitness_run (sweep)");
+    for (uint32_t i = 0; i < N; i++)
+        if (info[i].status != CTL_SIM_OK) {
+            set_error("simulation " + std::to_string(i) + " ended with status " + std::to_string(info[i].status));
+            return CTL_ERR_STEP_LIMIT;
+        }
     return CTL_OK;
 }
 

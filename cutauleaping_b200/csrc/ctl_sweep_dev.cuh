@@ -87,6 +87,8 @@ struct Run {
     uint32_t uniform_c;              // all simulations share row 0 of c
     uint32_t ssa_budget, dec_budget; // work per slot and round (SSA steps / decisions)
     uint32_t warp_local;             // 1: warp-local scheduling (no block rounds)
+    unsigned long long* sums;        // fitness mode: [sets][ns][s_out] sample sums, else null
+    uint32_t sum_threads, sum_prep;  // simulation -> parameter set (the reference's layout)
     const int32_t* __restrict__ X0;  // [n][S]
     const float* __restrict__ c;     // [n][R]
     uint32_t* __restrict__ out;      // [n][ns][s_out]
@@ -98,8 +100,8 @@ struct Run {
 // (consecutive threads hit consecutive banks).  G > 1: slot-contiguous
 // arrays of odd padded length (lanes of one group hit distinct banks).
 struct Layout {
-    uint32_t off_X, off_X1, off_a, off_K, off_tree, off_crit, off_c, off_state, off_list, off_grp;
-    uint32_t len_S, len_P, len_C, len_T;  // padded lengths (G > 1)
+    uint32_t off_X, off_X1, off_a, off_K, off_tree, off_crit, off_c, off_state, off_list, off_grp, off_last;
+    uint32_t len_S, len_P, len_C, len_T, len_O;  // padded lengths (G > 1)
 };
 
 // Per-slot scalars, one array each (index = slot).
@@ -388,6 +390,7 @@ struct Slot {
     uint32_t* K;
     uint8_t* crit;
     float* c;
+    uint32_t* last;  // fitness mode: the simulation's last recorded sample [s_out]
     int st;   // element stride of the slot arrays
     int cst;  // element stride of the rate constants (1 when shared by the block)
     __device__ __forceinline__ int32_t& x(int i) const { return X[i * st]; }
@@ -397,6 +400,7 @@ struct Slot {
     __device__ __forceinline__ uint32_t& k(int i) const { return K[i * st]; }
     __device__ __forceinline__ uint8_t& cr(int i) const { return crit[i * st]; }
     __device__ __forceinline__ float& cf(int i) const { return c[i * cst]; }
+    __device__ __forceinline__ uint32_t& lst(int i) const { return last[i * st]; }
 };
 
 // One reactant factor: X for coefficient 1, 0.5 X (X-1) for 2.
@@ -583,23 +587,58 @@ __device__ void update_after_fire(const Grp<G>& g, const Model& m, const Slot& s
     }
 }
 
+// Where a simulation's samples go: its own rows [ns][s_out] (dynamics), or,
+// in fitness mode, added into the 64-bit sums [ns][s_out] of its parameter
+// set (integer sums: exact and independent of the order simulations finish
+// in), with the last recorded row kept in the slot for the copy-forward.
+struct Out {
+    uint32_t* samples;
+    unsigned long long* sums;
+    __device__ __forceinline__ void put(const Slot& sl, uint32_t i, int so, int k, uint32_t v) const {
+        if (samples) {
+            samples[(size_t)i * so + k] = v;
+        } else {
+            atomicAdd(sums + (size_t)i * so + k, (unsigned long long)v);
+            sl.lst(k) = v;
+        }
+    }
+    __device__ __forceinline__ uint32_t get(const Slot& sl, uint32_t i, int so, int k) const {
+        return samples ? samples[(size_t)i * so + k] : sl.lst(k);
+    }
+};
+
+__device__ __forceinline__ Out out_of(const Run& run, uint32_t sim, size_t row_words) {
+    Out o;
+    if (run.sums) {
+        const uint32_t tp = run.sum_threads * run.sum_prep;
+        const uint32_t set = (sim / tp) * run.sum_threads + sim % run.sum_threads;
+        o.samples = nullptr;
+        o.sums = run.sums + (size_t)set * row_words;
+    } else {
+        o.samples = run.out + (size_t)sim * row_words;
+        o.sums = nullptr;
+    }
+    return o;
+}
+
 // A0 == 0 (tau.cu:1665-1697, 2165-2196): the reference copies the last
 // recorded sample forward (writing the current state first if none exists).
 template <int G>
 __device__ void finish_zero(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl,
-                            uint32_t* out, uint32_t& cursor) {
+                            const Out& out, uint32_t& cursor) {
     const int so = m.s_out;
     const uint32_t ns = (uint32_t)m.ns;
     if (!(run.flags & F_Q10_OFF)) {
         if (cursor == 0) {
-            for (int k = (int)g.lane; k < so; k += G) out[k] = (uint32_t)sl.x((int)m.cs[k]);
+            for (int k = (int)g.lane; k < so; k += G) out.put(sl, 0u, so, k, (uint32_t)sl.x((int)m.cs[k]));
             cursor = 1;
         }
+        // each lane copies its own columns k, which it wrote itself
         for (uint32_t i = cursor; i < ns; i++)
-            for (int k = (int)g.lane; k < so; k += G) out[(size_t)i * so + k] = out[(size_t)(cursor - 1) * so + k];
+            for (int k = (int)g.lane; k < so; k += G) out.put(sl, i, so, k, out.get(sl, cursor - 1, so, k));
     } else {
         for (uint32_t i = cursor; i < ns; i++)
-            for (int k = (int)g.lane; k < so; k += G) out[(size_t)i * so + k] = (uint32_t)sl.x((int)m.cs[k]);
+            for (int k = (int)g.lane; k < so; k += G) out.put(sl, i, so, k, (uint32_t)sl.x((int)m.cs[k]));
     }
     cursor = ns;
 }
@@ -645,7 +684,7 @@ __device__ void init_sim(const Grp<G>& g, const Model& m, const Run& run, const 
 // it hands off, one Cao tau-leap with critical reactions and rejection.
 template <int G>
 __device__ int decide_step(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl, Sim& st,
-                           uint32_t* out) {
+                           const Out& out) {
     const int S = m.S, R = m.R, so = m.s_out;
     const uint32_t ns = (uint32_t)m.ns;
     const uint32_t fl = run.flags;
@@ -785,7 +824,7 @@ __device__ int decide_step(const Grp<G>& g, const Model& m, const Run& run, cons
                 v = (uint32_t)xs + (ri > 0.0 ? (uint32_t)ri : 0u);
             else
                 v = (uint32_t)((int64_t)xs + (int64_t)ri);
-            out[(size_t)st.cursor * so + k] = v;
+            out.put(sl, st.cursor, so, k, v);
         }
         st.cursor++;
         st.t_next = st.cursor < ns ? m.tvec[st.cursor] : 0.0;
@@ -805,7 +844,7 @@ __device__ int decide_step(const Grp<G>& g, const Model& m, const Run& run, cons
 // EventualSSASteps / LightweightSSA (tau.cu:2099-2454): one direct-method step.
 template <int G>
 __device__ int ssa_step(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl, Sim& st,
-                        uint32_t* out) {
+                        const Out& out) {
     const int so = m.s_out;
     const uint32_t ns = (uint32_t)m.ns;
     const uint32_t lane = g.lane;
@@ -828,7 +867,7 @@ __device__ int ssa_step(const Grp<G>& g, const Model& m, const Run& run, const S
     const float dtf = -flog(u24f(wb)) / (float)A0;
     st.tl = st.tl + (double)dtf;
     while (st.cursor < ns && st.T + st.tl > st.t_next) {
-        for (int k = (int)lane; k < so; k += G) out[(size_t)st.cursor * so + k] = (uint32_t)sl.x((int)m.cs[k]);
+        for (int k = (int)lane; k < so; k += G) out.put(sl, st.cursor, so, k, (uint32_t)sl.x((int)m.cs[k]));
         st.cursor++;
         st.t_next = st.cursor < ns ? m.tvec[st.cursor] : 0.0;
     }
@@ -861,10 +900,11 @@ __device__ int ssa_step(const Grp<G>& g, const Model& m, const Run& run, const S
 }
 
 template <int G>
-__device__ void finish_sim(const Grp<G>& g, const Model& m, const Run& run, const Sim& st, uint32_t* out) {
+__device__ void finish_sim(const Grp<G>& g, const Model& m, const Run& run, const Sim& st, const Out& out) {
     const int so = m.s_out;
-    for (uint32_t i = st.cursor; i < (uint32_t)m.ns; i++)
-        for (int k = (int)g.lane; k < so; k += G) out[(size_t)i * so + k] = 0u;
+    if (out.samples)  // rows never reached read 0 (a sum gains nothing from them)
+        for (uint32_t i = st.cursor; i < (uint32_t)m.ns; i++)
+            for (int k = (int)g.lane; k < so; k += G) out.samples[(size_t)i * so + k] = 0u;
     const unsigned long long ftot = g.sum(st.fire);
     if (g.lane == 0) {
         ctl_sim_info inf;
@@ -930,6 +970,7 @@ __device__ __forceinline__ Slot slot_of(unsigned char* smem, const Layout& lay, 
         sl.tree = reinterpret_cast<double*>(smem + lay.off_tree) + j;
         sl.crit = reinterpret_cast<uint8_t*>(smem + lay.off_crit) + j;
         sl.c = reinterpret_cast<float*>(smem + lay.off_c) + (uniform_c ? 0 : j);
+        sl.last = reinterpret_cast<uint32_t*>(smem + lay.off_last) + j;
         sl.cst = uniform_c ? 1 : NS;
     } else {
         sl.st = 1;
@@ -940,6 +981,7 @@ __device__ __forceinline__ Slot slot_of(unsigned char* smem, const Layout& lay, 
         sl.tree = reinterpret_cast<double*>(smem + lay.off_tree) + (size_t)j * lay.len_T;
         sl.crit = reinterpret_cast<uint8_t*>(smem + lay.off_crit) + (size_t)j * lay.len_C;
         sl.c = reinterpret_cast<float*>(smem + lay.off_c) + (uniform_c ? 0 : (size_t)j * lay.len_P);
+        sl.last = reinterpret_cast<uint32_t*>(smem + lay.off_last) + (size_t)j * lay.len_O;
         sl.cst = 1;
     }
     return sl;
@@ -998,7 +1040,7 @@ __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layo
         const Slot sl = slot_of<G>(smem, lay, gi, NS, uni);
         Sim st;
         bool live = false, closed = false;
-        uint32_t* out = run.out;
+        Out out{nullptr, nullptr};
         for (;;) {
             if (!live && !closed) {
                 uint32_t sim = 0;
@@ -1009,7 +1051,7 @@ __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layo
                 } else {
                     init_sim<G>(g, m, run, sl, st, sim);
                     live = true;
-                    out = run.out + (size_t)st.sim * sim_stride;
+                    out = out_of(run, st.sim, sim_stride);
                 }
             }
             if (__all_sync(0xffffffffu, closed)) break;
@@ -1079,7 +1121,7 @@ __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layo
             const Slot sl = slot_of<G>(smem, lay, j, NS, uni);
             Sim st;
             load_sim<G>(g, sa, j, st);
-            uint32_t* out = run.out + (size_t)st.sim * sim_stride;
+            const Out out = out_of(run, st.sim, sim_stride);
             int res = CONT;
             if (is_ssa) {
                 for (uint32_t b = 0; b < run.ssa_budget; b++) {

@@ -217,6 +217,31 @@ ctl_status ctl_fitness_device(const uint32_t* d_samples, uint32_t ns, uint32_t s
                               uint32_t experiments, uint32_t repetitions, uint32_t threads,
                               uint32_t blocks, uint32_t p_rep, double* d_fitness, void* stream);
 
+/* ---- fitness mode without per-simulation samples ------------------------- */
+/* Replaces the run + calculateFitness pair of the reference's fitness mode
+ * (kernel.cu:347-423, 2phase_n-tau-leaping.cu:3324-3408) with a fused path:
+ * the sweep adds every recorded sample into 64-bit integer sums per
+ * parameter set instead of storing it (set of simulation gid =
+ * (gid / (threads*p_rep)) * threads + gid % threads, the reference's layout);
+ * the fitness then reads the sums.  Integer sums are exact, so the fitness
+ * equals the one computed from stored samples bit for bit.
+ * d_sums: [n / p_rep][ns][s_out] uint64, zeroed by the call. */
+ctl_status ctl_run_device_sums(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* d_X0,
+                               const float* d_c, uint32_t threads, uint32_t p_rep, uint64_t* d_sums,
+                               ctl_sim_info* d_info, void* stream);
+/* calculateFitness from the sums of ctl_run_device_sums (arguments as
+ * ctl_fitness_device). */
+ctl_status ctl_fitness_sums_device(const uint64_t* d_sums, uint32_t ns, uint32_t s_out,
+                                   const uint32_t* d_target, const uint8_t* d_experiment,
+                                   uint32_t experiments, uint32_t repetitions, uint32_t threads,
+                                   uint32_t blocks, uint32_t p_rep, double* d_fitness, void* stream);
+/* Host-buffer fitness mode: N = threads * blocks of the target, X0 [N][S],
+ * c [N][R] -> fitness [N] (entries of the N / p_rep parameter sets first,
+ * the rest 0, as ctl_fitness) and per-simulation records; CTL_ERR_STEP_LIMIT
+ * if a simulation ended early. */
+ctl_status ctl_fitness_run(ctl_model* m, const ctl_target* t, const ctl_run_cfg* cfg, const int32_t* X0,
+                           const float* c, double* fitness, ctl_sim_info* info);
+
 /* ---- surrogate MLP kernels (fitness-mode screening) ---------------------- */
 /* No reference counterpart: the reference evaluates every candidate by full
  * simulation (kernel.cu:365-423).  These are the tcgen05 kernels that train
