@@ -565,12 +565,7 @@ __device__ void update_after_fire(const Grp<G>& g, const Model& m, const Slot& s
         sl.pa(rr) = prop(m, sl, rr);
     }
     g.sync();
-    // Rebuild the stored levels when that takes no more lane iterations than
-    // updating the dependents' paths (equal trip counts in every group also
-    // keep the groups of a warp in lockstep); both give the same tree.
-    uint32_t full_it = 0;
-    for (int li = 0; li < m.nlev; li++) full_it += ((uint32_t)m.lev_count[li] + G - 1) / G;
-    if (full_it <= (uint32_t)m.nlev * ((nd + G - 1) / G)) {
+    if (nd >= (uint32_t)m.lev_count[0]) {  // touches about every bottom group: rebuild
         build_tree<G>(g, m, sl, 0);
         return;
     }

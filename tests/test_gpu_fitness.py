@@ -55,7 +55,7 @@ def _both_paths(net, threads, p_rep, E, REP, seed, **cfgkw):
     assert L.ctl_fitness_device(P(out.data_ptr()), ns, so, P(tg.data_ptr()), P(sw.data_ptr()), E, REP, threads,
                                 blocks, p_rep, P(fa.data_ptr()), P(stream)) == ctl.OK
     # per-set sums -> fitness
-    sums = torch.full((n // p_rep) * ns * so, -1, dtype=torch.int64, device="cuda")
+    sums = torch.full(((n // p_rep) * ns * so,), -1, dtype=torch.int64, device="cuda")
     info_b = torch.empty(n * 40, dtype=torch.uint8, device="cuda")
     assert L.ctl_run_device_sums(m._h, C.byref(cfg), n, P(X0.data_ptr()), P(c.data_ptr()), threads, p_rep,
                                  P(sums.data_ptr()), P(info_b.data_ptr()), P(stream)) == ctl.OK
