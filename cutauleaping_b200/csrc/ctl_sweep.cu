@@ -301,11 +301,14 @@ static const void* kernel_for(int G, int minb) {
 }
 
 // Lanes per simulation when the caller does not choose: about 16
-// reactions per lane (measured best for 64x128: G = 8; tiny networks: 1).
+// reactions per lane up to one warp (measured best for 64 x 128: G = 8;
+// tiny networks: 1), about 8 per lane beyond (512 x 1024: G = 128, 1.8x
+// the throughput of G = 32).
 static int heuristic_group(const HostTables& t) {
-    int g = t.P / 16;
+    const int g = t.P >= 1024 ? t.P / 8 : t.P / 16;
+    const int cap = t.P >= 1024 ? 256 : 32;
     int G = 1;
-    while (G < g && G < 32) G <<= 1;
+    while (G < g && G < cap) G <<= 1;
     return G;
 }
 
