@@ -138,12 +138,18 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
 // sigmoid(z) = 0.5 + 0.5 tanh(z / 2), one MUFU operation per element
 // (tanh.approx.f32, relative error about 2^-11, below the BF16 rounding that
 // follows).  Training and screening use the same form.
-__device__ __forceinline__ float sigm(float z) {
+__device__ __forceinline__ float tanh_hw(float x) {
     float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
-    return fmaf(0.5f, t, 0.5f);
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(x));
+    return t;
 }
-__device__ __forceinline__ float silu(float z) { return z * sigm(z); }
+__device__ __forceinline__ float sigm(float z) { return fmaf(0.5f, tanh_hw(0.5f * z), 0.5f); }
+// silu(z) = z sigmoid(z) = h tanh(h) + h with h = z / 2: one multiply, one
+// MUFU and one FMA per element.
+__device__ __forceinline__ float silu(float z) {
+    const float h = 0.5f * z;
+    return fmaf(h, tanh_hw(h), h);
+}
 __device__ __forceinline__ float silu_grad(float z) {
     const float s = sigm(z);
     return s * (1.0f + z * (1.0f - s));
@@ -357,8 +363,8 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
 //     slot's epilogue overlaps the other slot's MMAs.
 // TMEM: 512 columns, 256 per slot.
 constexpr int SC_BK = 32, SC_STAGES = 5, SC_HID = 256, SC_LAYERS = 5;
-constexpr int SC_EPI = 256;                       // epilogue threads per slot
-constexpr int SC_THREADS = 2 * SC_EPI + 64;       // + producer and MMA warps
+constexpr int SC_EPI = 512;                       // epilogue threads (16 warps)
+constexpr int SC_THREADS = SC_EPI + 64;           // + producer and MMA warps
 constexpr int SC_A_BYTES = 128 * SC_HID * 2;      // one slot's activation tile
 constexpr int SC_STAGE_BYTES = SC_HID * SC_BK * 2;
 constexpr int SC_CONST_BYTES = 16384;             // biases, output scaling, target (when it fits)
@@ -396,6 +402,20 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+// 32 columns of the accumulator into registers; tmem_wait() makes them
+// valid, so a second load can be in flight while the first is processed.
+__device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     uint32_t r[32];
     asm volatile(
@@ -422,20 +442,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
-// Named barrier 1 + slot over one slot's 256 epilogue threads, and the same
-// barrier as a vote: true when every thread of the slot passes true.
-__device__ __forceinline__ void epi_sync(uint32_t id) {
-    asm volatile("bar.sync %0, 256;" ::"r"(id) : "memory");
-}
-__device__ __forceinline__ bool epi_all(uint32_t id, bool v) {
+// Named barrier 1 over the 512 epilogue threads, and the same barrier as a
+// vote: true when every epilogue thread passes true.
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 512;" ::: "memory"); }
+__device__ __forceinline__ bool epi_all(bool v) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred a, b;\n\t"
         "setp.ne.u32 a, %1, 0;\n\t"
-        "bar.red.and.pred b, %2, 256, a;\n\t"
+        "bar.red.and.pred b, 1, 512, a;\n\t"
         "selp.u32 %0, 1, 0, b;\n\t}"
         : "=r"(r)
-        : "r"((uint32_t)v), "r"(id)
+        : "r"((uint32_t)v)
         : "memory");
     return r != 0;
 }
@@ -451,16 +469,16 @@ __device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// Layer-0 input columns [32h, 32h + 32) of row r of the tile: scaled log
-// parameters in [-1, 1], scaled time, zeros (the same FP32 operations as
-// surrogate.make_inputs).
-__device__ void sc_build_input(const Screen& p, uint8_t* A, int r, int h, uint32_t row) {
-    float x[32];
-    const int c0 = 32 * h;
+// Layer-0 input columns [16 part, 16 part + 16) of row r of the tile:
+// scaled log parameters in [-1, 1], scaled time, zeros (the same FP32
+// operations as surrogate.make_inputs).
+__device__ void sc_build_input(const Screen& p, uint8_t* A, int r, int part, uint32_t row) {
+    float x[16];
+    const int c0 = 16 * part;
     const bool live = row < p.n_rows;
     const uint32_t cand = live ? row / p.ns : 0u, ti = live ? row % p.ns : 0u;
 #pragma unroll
-    for (int q = 0; q < 32; q++) {
+    for (int q = 0; q < 16; q++) {
         const int j = c0 + q;
         float v = 0.0f;
         if (live && j < p.n_par) {
@@ -472,7 +490,7 @@ __device__ void sc_build_input(const Screen& p, uint8_t* A, int r, int h, uint32
         x[q] = v;
     }
 #pragma unroll
-    for (int kb = 0; kb < 4; kb++) {
+    for (int kb = 0; kb < 2; kb++) {
         uint4 v;
         v.x = pack_bf2(x[kb * 8 + 0], x[kb * 8 + 1]);
         v.y = pack_bf2(x[kb * 8 + 2], x[kb * 8 + 3]);
@@ -493,7 +511,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
     __shared__ __align__(8) uint64_t full[SC_STAGES], empty[SC_STAGES], acc_full[2], a_ready[2], drain;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
-    __shared__ float s_acc[2][132];
+    __shared__ float s_acc[132];
     uint8_t* stage = smem + 2 * SC_A_BYTES;
     // per-CTA constants in shared memory: biases [4*256 + out_w], y_mean [S],
     // y_std [S], and the target [ns][S] when it fits
@@ -525,7 +543,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = threadIdx.x; i < 2 * 132; i += SC_THREADS) (&s_acc[0][0])[i] = 0.0f;
+    for (int i = threadIdx.x; i < 132; i += SC_THREADS) s_acc[i] = 0.0f;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      ::"r"(smem_u32(&tmem_slot)), "r"(2 * SC_HID));
@@ -609,83 +627,94 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
             mbar_wait(&drain, 0u, nullptr);
         }
     } else {
-        // ---- epilogue of slot e = warp / 8: warp w owns rows 32(w%4).. (its
-        // TMEM lane quadrant) and column half (w/4)%2; thread r = row ----
-        const uint32_t e = (uint32_t)warp >> 3;
-        const uint32_t bar_id = 1u + e;
-        const int q = warp & 3, h = (warp >> 2) & 1;
+        // ---- epilogue warps 0-15, in the MMA issuer's order (per tile pair
+        // and layer, slot 0 then slot 1): warp w owns rows 32(w%4).. (its TMEM
+        // lane quadrant) and columns [64 part, 64 part + 64), part = w / 4 ----
+        const int q = warp & 3, part = warp >> 2;
         const int r = q * 32 + lane;
-        const int et = (int)threadIdx.x - (int)e * SC_EPI;  // 0..255 within the slot
-        uint8_t* A = smem + e * SC_A_BYTES;
-        float* acc_c = s_acc[e];
-        const uint32_t tbase = tmem + e * SC_HID + ((uint32_t)(q * 32) << 16);
-        uint32_t nacc = 0;
+        const int et = (int)threadIdx.x;  // 0..511
+        uint32_t nacc[2] = {0u, 0u};
         bool ok = true;
-        for (uint32_t i = e; i < my && ok; i += 2) {
-            const uint32_t t = blockIdx.x + i * gridDim.x;
-            const uint32_t row = t * 128u + (uint32_t)r;
-            sc_build_input(p, A, r, h, row);
-            fence_async_smem();
-            tc_fence_before();
-            mbar_arrive(&a_ready[e]);
-            for (int l = 0; l < SC_LAYERS; l++) {
-                bool got = mbar_wait(&acc_full[e], nacc & 1u, p.err);
-                got = epi_all(bar_id, got && !*(volatile int*)&abort_flag);  // uniform over the slot
-                nacc++;
-                if (!got) { ok = false; break; }
-                tc_fence_after();
-                if (l < SC_LAYERS - 1) {
-                    const float* b = c_bias + l * SC_HID;
-                    for (int c = 128 * h; c < 128 * h + 128; c += 32) {
-                        float v[32];
-                        tmem_ld32(tbase + (uint32_t)c, v);
-                        const float4* b4 = reinterpret_cast<const float4*>(b + c);
+        for (uint32_t i0 = 0; i0 < my && ok; i0 += 2) {
+            for (uint32_t i = i0; i < i0 + 2 && i < my; i++) {  // inputs of the pair's tiles
+                const uint32_t row = (blockIdx.x + i * gridDim.x) * 128u + (uint32_t)r;
+                sc_build_input(p, smem + (i & 1u) * SC_A_BYTES, r, part, row);
+                fence_async_smem();
+                tc_fence_before();
+                mbar_arrive(&a_ready[i & 1u]);
+            }
+            for (int l = 0; l < SC_LAYERS && ok; l++) {
+                for (uint32_t i = i0; i < i0 + 2 && i < my; i++) {
+                    const uint32_t e = i & 1u;
+                    const uint32_t t = blockIdx.x + i * gridDim.x;
+                    const uint32_t row = t * 128u + (uint32_t)r;
+                    uint8_t* A = smem + e * SC_A_BYTES;
+                    const uint32_t tbase = tmem + e * SC_HID + ((uint32_t)(q * 32) << 16);
+                    bool got = mbar_wait(&acc_full[e], nacc[e] & 1u, p.err);
+                    got = epi_all(got && !*(volatile int*)&abort_flag);  // uniform over the epilogue
+                    nacc[e]++;
+                    if (!got) { ok = false; break; }
+                    tc_fence_after();
+                    if (l < SC_LAYERS - 1) {
+                        const float* b = c_bias + l * SC_HID;
+                        const int c0 = 64 * part;
+                        uint32_t ra[32], rb[32];
+                        tmem_ld32_issue(tbase + (uint32_t)c0, ra);
+                        tmem_wait();
+                        tmem_ld32_issue(tbase + (uint32_t)(c0 + 32), rb);  // in flight during the first chunk
 #pragma unroll
-                        for (int k = 0; k < 4; k++) {  // 8 columns -> one 16-byte store
-                            const float4 ba = b4[2 * k], bb = b4[2 * k + 1];
-                            const float* u = v + 8 * k;
-                            uint4 o;
-                            o.x = pack_bf2(silu(u[0] + ba.x), silu(u[1] + ba.y));
-                            o.y = pack_bf2(silu(u[2] + ba.z), silu(u[3] + ba.w));
-                            o.z = pack_bf2(silu(u[4] + bb.x), silu(u[5] + bb.y));
-                            o.w = pack_bf2(silu(u[6] + bb.z), silu(u[7] + bb.w));
-                            *reinterpret_cast<uint4*>(A + canon(r, c + 8 * k, 128)) = o;
-                        }
-                    }
-                    fence_async_smem();
-                    tc_fence_before();
-                    mbar_arrive(&a_ready[e]);
-                } else {
-                    // fitness terms of this row: sum_s |target - mean| (/ target when
-                    // nonzero), 16-column chunks alternating between the two halves
-                    const float* b = c_bias + (SC_LAYERS - 1) * SC_HID;
-                    float acc = 0.0f;
-                    const uint32_t ti = row % p.ns;
-                    for (int c = 16 * h; c < p.S; c += 32) {
-                        float v[16];
-                        tmem_ld16(tbase + (uint32_t)c, v);
+                        for (int half = 0; half < 2; half++) {
+                            if (half == 1) tmem_wait();
+                            const uint32_t* rr = half == 0 ? ra : rb;
+                            const int c = c0 + 32 * half;
+                            const float4* b4 = reinterpret_cast<const float4*>(b + c);
 #pragma unroll
-                        for (int j = 0; j < 16; j++) {
-                            const int s_ = c + j;
-                            if (s_ < p.S && row < p.n_rows) {
-                                const float mean = (v[j] + b[s_]) * c_ys[s_] + c_ym[s_];
-                                const float tg = tgt[(size_t)ti * p.S + s_];
-                                float d = fabsf(tg - mean);
-                                if (tg != 0.0f) d = d / tg;
-                                acc += d;
+                            for (int k = 0; k < 4; k++) {  // 8 columns -> one 16-byte store
+                                const float4 ba = b4[2 * k], bb = b4[2 * k + 1];
+                                const uint32_t* u = rr + 8 * k;
+                                uint4 o;
+                                o.x = pack_bf2(silu(__uint_as_float(u[0]) + ba.x), silu(__uint_as_float(u[1]) + ba.y));
+                                o.y = pack_bf2(silu(__uint_as_float(u[2]) + ba.z), silu(__uint_as_float(u[3]) + ba.w));
+                                o.z = pack_bf2(silu(__uint_as_float(u[4]) + bb.x), silu(__uint_as_float(u[5]) + bb.y));
+                                o.w = pack_bf2(silu(__uint_as_float(u[6]) + bb.z), silu(__uint_as_float(u[7]) + bb.w));
+                                *reinterpret_cast<uint4*>(A + canon(r, c + 8 * k, 128)) = o;
                             }
                         }
+                        fence_async_smem();
+                        tc_fence_before();
+                        mbar_arrive(&a_ready[e]);
+                    } else {
+                        // fitness terms of this row: sum_s |target - mean| (/ target when
+                        // nonzero), 16-column chunks spread over the four column parts
+                        const float* b = c_bias + (SC_LAYERS - 1) * SC_HID;
+                        float acc = 0.0f;
+                        const uint32_t ti = row % p.ns;
+                        for (int c = 16 * part; c < p.S; c += 64) {
+                            float v[16];
+                            tmem_ld16(tbase + (uint32_t)c, v);
+#pragma unroll
+                            for (int j = 0; j < 16; j++) {
+                                const int s_ = c + j;
+                                if (s_ < p.S && row < p.n_rows) {
+                                    const float mean = (v[j] + b[s_]) * c_ys[s_] + c_ym[s_];
+                                    const float tg = tgt[(size_t)ti * p.S + s_];
+                                    float d = fabsf(tg - mean);
+                                    if (tg != 0.0f) d = d / tg;
+                                    acc += d;
+                                }
+                            }
+                        }
+                        tc_fence_before();
+                        const uint32_t cand0 = (t * 128u) / p.ns;
+                        if (row < p.n_rows && acc != 0.0f) atomicAdd(&s_acc[row / p.ns - cand0], acc);
+                        epi_sync();
+                        const uint32_t last = (min(t * 128u + 127u, p.n_rows - 1u)) / p.ns;
+                        if ((uint32_t)et <= last - cand0 && t * 128u < p.n_rows) {
+                            atomicAdd(&p.fit[cand0 + et], (double)s_acc[et]);
+                            s_acc[et] = 0.0f;
+                        }
+                        epi_sync();
                     }
-                    tc_fence_before();
-                    const uint32_t cand0 = (t * 128u) / p.ns;
-                    if (row < p.n_rows) atomicAdd(&acc_c[row / p.ns - cand0], acc);
-                    epi_sync(bar_id);
-                    const uint32_t last = (min(t * 128u + 127u, p.n_rows - 1u)) / p.ns;
-                    if ((uint32_t)et <= last - cand0 && t * 128u < p.n_rows) {
-                        atomicAdd(&p.fit[cand0 + et], (double)acc_c[et]);
-                        acc_c[et] = 0.0f;
-                    }
-                    epi_sync(bar_id);
                 }
             }
         }
