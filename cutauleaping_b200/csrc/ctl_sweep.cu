@@ -28,7 +28,10 @@
 #include <cfloat>
 #include <cstdint>
 #include <cstring>
+#include <chrono>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "ctl_internal.h"
 
@@ -509,7 +512,7 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
                                 const float* dc, uint32_t* dout, ctl_sim_info* dinfo,
                                 cudaStream_t stream, const LaunchPlan& pl, const DeviceCopy& d,
                                 unsigned long long* sums = nullptr, uint32_t sum_threads = 1,
-                                uint32_t sum_prep = 1) {
+                                uint32_t sum_prep = 1, uint32_t* done = nullptr, uint32_t done_shift = 0) {
     dev::Run run;
     run.seed = cfg->seed;
     run.eps = cfg->eps;
@@ -530,6 +533,8 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.sums = sums;
     run.sum_threads = sum_threads;
     run.sum_prep = sum_prep;
+    run.done = done;
+    run.done_shift = done_shift;
     run.info = dinfo;
     run.queue = d.ctrl;
     dev::Model dm = make_dev_model(m, d, cfg->flags);
@@ -662,32 +667,90 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
     LaunchPlan pl;
     if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;
     const size_t bx = (size_t)n * t.S * 4, bc = (size_t)n * t.R * 4;
-    const size_t bo = (size_t)n * t.ns * t.s_out * 4, bi = (size_t)n * sizeof(ctl_sim_info);
+    const size_t row = (size_t)t.ns * t.s_out * 4, bo = (size_t)n * row, bi = (size_t)n * sizeof(ctl_sim_info);
     keep_pool_memory(cfg->device);
-    cudaStream_t s;
+    // Copy/compute overlap: the batch is cut into up to 16 chunks of 2^shift
+    // simulations; the kernel counts finished simulations per chunk (after a
+    // device-scope fence) and each complete chunk's rows are copied back on a
+    // second stream while the sweep goes on.
+    uint32_t shift = 0;
+    while (((uint64_t)n >> shift) > 16) shift++;
+    const uint32_t nch = (uint32_t)(((uint64_t)n + (1ull << shift) - 1) >> shift);
+    const bool overlap = bo >= ((size_t)64 << 20) && nch > 1;
+    cudaStream_t s, cs;
     CTL_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    void *dx = nullptr, *dc = nullptr, *dout = nullptr, *dinf = nullptr;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamDestroy(s);
+        return cuda_fail(cudaErrorMemoryAllocation, "ctl_run (copy stream)");
+    }
+    void *dx = nullptr, *dc = nullptr, *dout = nullptr, *dinf = nullptr, *ddone = nullptr;
+    uint32_t* hdone = nullptr;
     cudaError_t e = cudaMallocAsync(&dx, bx, s);
     if (e == cudaSuccess) e = cudaMallocAsync(&dc, bc, s);
     if (e == cudaSuccess) e = cudaMallocAsync(&dout, bo, s);
     if (e == cudaSuccess) e = cudaMallocAsync(&dinf, bi, s);
+    if (e == cudaSuccess && overlap) e = cudaMallocAsync(&ddone, (size_t)nch * 4, s);
+    if (e == cudaSuccess && overlap) e = cudaMallocHost(reinterpret_cast<void**>(&hdone), (size_t)nch * 4);
+    if (e == cudaSuccess && overlap) e = cudaMemsetAsync(ddone, 0, (size_t)nch * 4, s);
+    if (e == cudaSuccess && overlap) {  // the copy stream starts after the counters are zeroed
+        cudaEvent_t zeroed;
+        e = cudaEventCreateWithFlags(&zeroed, cudaEventDisableTiming);
+        if (e == cudaSuccess) {
+            e = cudaEventRecord(zeroed, s);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, zeroed, 0);
+            cudaEventDestroy(zeroed);
+        }
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(dx, X0, bx, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dc, c, bc, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
         st = enqueue_sweep(m, cfg, n, static_cast<int32_t*>(dx), static_cast<float*>(dc),
-                           static_cast<uint32_t*>(dout), static_cast<ctl_sim_info*>(dinf), s, pl, *d);
+                           static_cast<uint32_t*>(dout), static_cast<ctl_sim_info*>(dinf), s, pl, *d, nullptr, 1, 1,
+                           static_cast<uint32_t*>(ddone), shift);
         if (st != CTL_OK) e = cudaErrorLaunchFailure;
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(samples, dout, bo, cudaMemcpyDeviceToHost, s);
+    std::vector<char> copied(nch, 0);
+    if (e == cudaSuccess && overlap) {
+        // poll the counters until the sweep ends, copying finished chunks
+        while (e == cudaSuccess) {
+            const cudaError_t q = cudaStreamQuery(s);
+            if (q == cudaSuccess) break;  // the rest is copied below
+            if (q != cudaErrorNotReady) { e = q; break; }
+            if ((e = cudaMemcpyAsync(hdone, ddone, (size_t)nch * 4, cudaMemcpyDeviceToHost, cs)) != cudaSuccess) break;
+            if ((e = cudaStreamSynchronize(cs)) != cudaSuccess) break;
+            for (uint32_t j = 0; j < nch && e == cudaSuccess; j++) {
+                const uint64_t lo = (uint64_t)j << shift, hi = std::min<uint64_t>(n, lo + (1ull << shift));
+                if (!copied[j] && hdone[j] == (uint32_t)(hi - lo)) {
+                    e = cudaMemcpyAsync(reinterpret_cast<unsigned char*>(samples) + lo * row,
+                                        static_cast<unsigned char*>(dout) + lo * row, (hi - lo) * row,
+                                        cudaMemcpyDeviceToHost, cs);
+                    copied[j] = 1;
+                }
+            }
+            if (e == cudaSuccess) std::this_thread::sleep_for(std::chrono::microseconds(200));
+        }
+    }
+    for (uint32_t j = 0; j < nch && e == cudaSuccess; j++) {  // chunks not yet copied, after the sweep
+        const uint64_t lo = (uint64_t)j << shift, hi = std::min<uint64_t>(n, lo + (1ull << shift));
+        if (!copied[j])
+            e = cudaMemcpyAsync(reinterpret_cast<unsigned char*>(samples) + lo * row,
+                                static_cast<unsigned char*>(dout) + lo * row, (hi - lo) * row,
+                                cudaMemcpyDeviceToHost, s);
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(info, dinf, bi, cudaMemcpyDeviceToHost, s);
+    const cudaError_t e3 = cudaStreamSynchronize(cs);  // copies in flight end before the buffers go
     if (dx) cudaFreeAsync(dx, s);
     if (dc) cudaFreeAsync(dc, s);
     if (dout) cudaFreeAsync(dout, s);
     if (dinf) cudaFreeAsync(dinf, s);
-    cudaError_t e2 = cudaStreamSynchronize(s);
+    if (ddone) cudaFreeAsync(ddone, s);
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    if (hdone) cudaFreeHost(hdone);
+    cudaStreamDestroy(cs);
     cudaStreamDestroy(s);
     if (st != CTL_OK) return st;
     if (e != cudaSuccess) return cuda_fail(e, "ctl_run");
+    if (e3 != cudaSuccess) return cuda_fail(e3, "ctl_run (copies)");
     if (e2 != cudaSuccess) return cuda_fail(e2, "ctl_run (sweep)");
     for (uint32_t i = 0; i < n; i++)
         if (info[i].status != CTL_SIM_OK) {

@@ -89,6 +89,8 @@ struct Run {
     uint32_t warp_local;             // 1: warp-local scheduling (no block rounds)
     unsigned long long* sums;        // fitness mode: [sets][ns][s_out] sample sums, else null
     uint32_t sum_threads, sum_prep;  // simulation -> parameter set (the reference's layout)
+    uint32_t* done;                  // optional: finished simulations per chunk of 2^done_shift
+    uint32_t done_shift;
     const int32_t* __restrict__ X0;  // [n][S]
     const float* __restrict__ c;     // [n][R]
     uint32_t* __restrict__ out;      // [n][ns][s_out]
@@ -912,6 +914,11 @@ __device__ void finish_sim(const Grp<G>& g, const Model& m, const Run& run, cons
         inf.rejections = st.rej;
         inf.pad = 0;
         run.info[st.sim] = inf;
+    }
+    if (run.done) {  // publish: this simulation's rows and record are complete
+        __threadfence();
+        g.sync();
+        if (g.lane == 0) atomicAdd(run.done + (st.sim >> run.done_shift), 1u);
     }
 }
 

@@ -120,3 +120,28 @@ def test_multiwarp_groups_bit_exact():
             assert np.array_equal(out, out_o), f"G={G} threads={threads} sched={sched}"
             assert same_info(info, info_o) is None, f"G={G} threads={threads} sched={sched}"
             assert m.launch_info(net.n, group=G, threads=threads).group == G
+
+
+def test_host_run_with_overlapped_copies_matches_device_run():
+    """ctl_run copies finished chunks back while the sweep runs (batches with
+    64 MB of samples or more): its rows and records equal a device-resident
+    run's, and sampled rows equal the oracle's."""
+    import torch
+    from cutauleaping_b200 import inputs
+    net = inputs.synthetic(64, 128, 2304, seed=0, t_end=0.4, samples=200)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    assert 2304 * 200 * 64 * 4 >= 64 << 20
+    out_h, info_h = m.run(net.X0, net.c, seed=3)
+    X0 = torch.as_tensor(np.ascontiguousarray(net.X0, np.int32), device="cuda")
+    c = torch.as_tensor(np.ascontiguousarray(net.c, np.float32), device="cuda")
+    out = torch.empty((net.n, 200, 64), dtype=torch.int32, device="cuda")
+    info = torch.empty((net.n, 40), dtype=torch.uint8, device="cuda")
+    m.run_device(net.n, X0.data_ptr(), c.data_ptr(), out.data_ptr(), info.data_ptr(),
+                 torch.cuda.current_stream().cuda_stream,
+                 ctl.run_cfg(seed=3, uniform_rates=int(bool((net.c == net.c[0]).all()))))
+    torch.cuda.synchronize()
+    assert np.array_equal(out_h, out.cpu().numpy().view(np.uint32))
+    assert np.array_equal(info_h.view(np.uint8).reshape(net.n, 40), info.cpu().numpy())
+    sub = net.subset(slice(2300, 2304))
+    out_o, info_o = oracle_run(sub, seed=3, sim_base=2300)
+    assert np.array_equal(out_h[2300:2304], out_o)
