@@ -447,6 +447,12 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     pl.dec_budget = cfg->dec_budget;
     pl.sched = cfg->sched > 0 ? cfg->sched : 1;
     int G = cfg->group > 0 ? cfg->group : heuristic_group(t);
+    if (cfg->group <= 0) {  // small batches: more lanes per simulation so that every SM gets warps
+        DevAttr da0;
+        if (device_attr(cfg->device, da0) != CTL_OK) return CTL_ERR_CUDA;
+        const int gmax = std::min(t.P, 32);
+        while (G < gmax && (uint64_t)n * G < (uint64_t)2 * 256 * da0.sm_count) G <<= 1;
+    }
     if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32 && G != 64 && G != 128 && G != 256) {
         set_error("group must be a power of two from 1 to 256");
         return CTL_ERR_ARG;
@@ -463,12 +469,14 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     if (device_attr(dev_id, da) != CTL_OK) return CTL_ERR_CUDA;
     KernAttr ka;
     const bool uni = cfg->uniform_rates != 0;
-    // Register budget: as many resident blocks as the slot memory of a full
-    // 256-thread block allows (2 or 3; 4 only when chosen or tuned).
+    // Register budget: for groups of 8 lanes or more, as many resident
+    // blocks as the slot memory of a full 256-thread block allows (2 or 3);
+    // smaller groups keep 2 (their spills cost more than the occupancy
+    // gains: Schlogl at G = 1, 62k vs 56k sims/s); 4 only when chosen or tuned.
     int minb = cfg->min_blocks;
     if (minb <= 0) {
         const size_t full = slot_layout(t, G, 256 / G, uni, pl.lay, sums);
-        minb = 3 * (full + 1024) <= (size_t)da.smem_optin + 1024 ? 3 : 2;
+        minb = G >= 8 && 3 * (full + 1024) <= (size_t)da.smem_optin + 1024 ? 3 : 2;
     }
     if (ctl_status st = kernel_attr(dev_id, G, minb, ka); st != CTL_OK) return st;
     const size_t smem_max = ka.dyn_max;

@@ -94,8 +94,8 @@ typedef struct {
     int32_t dec_budget;   /* leap decisions per simulation and round (0 = 2)           */
     int32_t min_blocks;   /* register budget: kernel variant compiled for this many resident
                              256-thread blocks per SM (2: up to 128 registers per thread,
-                             3: 80, 4: 64); 0 = library choice (autotuned, else 3 when
-                             three full blocks' slots fit in shared memory, else 2)   */
+                             3: 80, 4: 64); 0 = library choice (autotuned, else 3 for
+                             groups of 8+ lanes whose slots fit three blocks, else 2) */
     int32_t sched;        /* scheduling: 1 = block rounds regrouping simulations by phase,
                              2 = warp-local (no block barriers); 0 = library choice   */
 } ctl_run_cfg;
