@@ -315,6 +315,7 @@ def main():
     ap.add_argument("--sched", type=int, default=0,
                     help="scheduling: 1 block regrouping rounds, 2 warp-local (0 = library choice)")
     ap.add_argument("--autotune", action="store_true", help="measure launch shapes before timing")
+    ap.add_argument("--no-autotune", action="store_true", help="config 3: library default shapes")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     a = ap.parse_args()
@@ -373,8 +374,9 @@ def main():
         c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).to(dev)
         out = torch.empty((n, model.ns, model.s_out), dtype=torch.int32, device=dev)
         info = torch.empty((n, 40), dtype=torch.uint8, device=dev)
-        if a.autotune:
-            # the sample must fill the GPU like the full batch does: a quarter of it, >= 16384
+        if a.autotune or (a.config == 3 and not a.no_autotune):
+            # config 3 is defined with an autotuned block shape; the sample must
+            # fill the GPU like the full batch does: a quarter of it, >= 16384
             model.autotune(n, X0.data_ptr(), c.data_ptr(), sample=min(n, max(16384, n // 4)), cfg=cfg)
         li = model.launch_info(n, cfg)
         graph = model.graph(n, X0.data_ptr(), c.data_ptr(), out.data_ptr(), info.data_ptr(),
@@ -504,8 +506,9 @@ def main():
                                    "blocks": pt["li"].blocks, "slots_per_block": pt["li"].slots_per_block,
                                    "smem_bytes": pt["li"].smem_bytes, "regs": pt["li"].regs_per_thread,
                                    "min_blocks": pt["li"].min_blocks, "sched": pt["li"].sched,
+                                   "ssa_budget": pt["li"].ssa_budget, "dec_budget": pt["li"].dec_budget,
                                    "blocks_per_sm": pt["li"].blocks_per_sm} for pt in parts],
-                       "autotuned": bool(a.autotune),
+                       "autotuned": bool(a.autotune or (a.config == 3 and not a.no_autotune)),
                        "parallelism": f"dp{world} (independent simulations per rank)"},
             "roofline": {"bound": "hbm", "achieved": abytes / (ms * 1e-3) / 1e9,
                          "peak": hbm_peak, "unit": "GB/s",

@@ -66,7 +66,8 @@ class LaunchInfo(C.Structure):
     _fields_ = [("group", C.c_int32), ("threads", C.c_int32), ("blocks", C.c_int32),
                 ("slots_per_block", C.c_int32), ("smem_bytes", C.c_int32),
                 ("regs_per_thread", C.c_int32), ("blocks_per_sm", C.c_int32),
-                ("sm_count", C.c_int32), ("min_blocks", C.c_int32), ("sched", C.c_int32)]
+                ("sm_count", C.c_int32), ("min_blocks", C.c_int32), ("sched", C.c_int32),
+                ("ssa_budget", C.c_int32), ("dec_budget", C.c_int32)]
 
 
 class CtlError(RuntimeError):

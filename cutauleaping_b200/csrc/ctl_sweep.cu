@@ -628,6 +628,8 @@ extern "C" ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uin
     li->sm_count = pl.sm_count;
     li->min_blocks = pl.minb;
     li->sched = pl.sched;
+    li->ssa_budget = pl.ssa_budget > 0 ? pl.ssa_budget : 8;
+    li->dec_budget = pl.dec_budget > 0 ? pl.dec_budget : 2;
     return CTL_OK;
 }
 

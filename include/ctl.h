@@ -112,6 +112,7 @@ typedef struct {
     int32_t smem_bytes, regs_per_thread, blocks_per_sm, sm_count;
     int32_t min_blocks;   /* register budget of the kernel variant (ctl_run_cfg.min_blocks) */
     int32_t sched;        /* scheduling mode (ctl_run_cfg.sched) */
+    int32_t ssa_budget, dec_budget;  /* work per simulation and round */
 } ctl_launch_info;
 
 /* ---- errors ------------------------------------------------------------ */
