@@ -138,12 +138,12 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def cpu_reference(net, desc, steps, warmup, sample_s=10.0, threads=None):
+def cpu_reference(net, desc, steps, warmup, sample_s=10.0, threads=None, flags=0):
     """The reference routine on the host: oracle port, all host threads,
     bounded samples of the same workload.  Returns (sims/s, firings/s, meta)."""
     import oracle
     threads = threads or os.cpu_count() or 1
-    m = oracle.OracleModel(net.left, net.right, net.feed, net.tvec, net.cs, seed=1)
+    m = oracle.OracleModel(net.left, net.right, net.feed, net.tvec, net.cs, seed=1, flags=flags)
     c32 = net.c.astype(np.float32)
     # size the sample so that one step takes about `sample_s` seconds
     k = min(net.n, max(threads, 64))
@@ -164,14 +164,14 @@ def cpu_reference(net, desc, steps, warmup, sample_s=10.0, threads=None):
         "cores": threads, "sample": f"{k} of the {net.n} simulations per step ({desc.split(',')[0]})"}
 
 
-def cpu_reference_segments(segs, steps, warmup):
+def cpu_reference_segments(segs, steps, warmup, flags=0):
     """CPU port over every segment: sims/s of the whole step = total sims /
     sum of per-segment times (each measured on a bounded sample)."""
     tot_n, tot_t, tot_f, meta = 0, 0.0, 0.0, None
     budget = 10.0 / len(segs)
     samples = []
     for net, desc in segs:
-        v, fv, meta = cpu_reference(net, desc, steps, warmup, sample_s=budget)
+        v, fv, meta = cpu_reference(net, desc, steps, warmup, sample_s=budget, flags=flags)
         tot_n += net.n
         tot_t += net.n / v
         tot_f += fv * (net.n / v)
@@ -314,6 +314,7 @@ def main():
                     help="register budget of the sweep kernel: 2, 3 or 4 resident blocks (0 = library choice)")
     ap.add_argument("--sched", type=int, default=0,
                     help="scheduling: 1 block regrouping rounds, 2 warp-local (0 = library choice)")
+    ap.add_argument("--flags", type=int, default=0, help="run flags (quirk switches; 1 = forced SSA)")
     ap.add_argument("--autotune", action="store_true", help="measure launch shapes before timing")
     ap.add_argument("--no-autotune", action="store_true", help="config 3: library default shapes")
     ap.add_argument("--no-e2e", action="store_true")
@@ -341,7 +342,7 @@ def main():
     if a.impl == "reference":
         if rank != 0:
             return
-        v, fv, meta = cpu_reference_segments(segs, a.steps, a.warmup)
+        v, fv, meta = cpu_reference_segments(segs, a.steps, a.warmup, a.flags)
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": "sims/s",
             "firings_per_s": fv, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
@@ -369,7 +370,7 @@ def main():
         model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
         n = net.n
         cfg = ctl.run_cfg(seed=1 + si, sim_base=rank * n, device=local, group=a.group, threads=a.threads,
-                          min_blocks=a.min_blocks, sched=a.sched, uniform_rates=int(bool((net.c == net.c[0]).all())))
+                          min_blocks=a.min_blocks, sched=a.sched, flags=a.flags, uniform_rates=int(bool((net.c == net.c[0]).all())))
         X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).to(dev)
         c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).to(dev)
         out = torch.empty((n, model.ns, model.s_out), dtype=torch.int32, device=dev)
@@ -489,7 +490,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        v, fv, meta = cpu_reference_segments(segs, 1, 0)
+        v, fv, meta = cpu_reference_segments(segs, 1, 0, a.flags)
         cpu = {"value": v, "unit": "sims/s", "cores": meta["cores"], "kind": "port",
                "sample": meta["sample"], "firings_per_s": fv}
 
