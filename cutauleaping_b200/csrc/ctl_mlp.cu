@@ -347,25 +347,26 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
 //
 // Screening scores candidates by the surrogate's ensemble mean: rows are
 // (candidate, sample instant) pairs, row = cand * ns + ti.  One persistent
-// CTA per SM works on two 128-row tiles at a time (ping-pong) and keeps each
-// tile's activations in shared memory for all five layers, so HBM sees only
-// the candidates' parameters and one fitness word per candidate:
-//   * warps 0-7 / 8-15 (epilogue of tile slot 0 / 1): build the layer-0 input
-//     rows, then per layer read the slot's TMEM accumulator (warp w owns rows
+// CTA per SM works on two 128-row tiles at a time and keeps their
+// activations in shared memory for all five layers, so HBM sees only the
+// candidates' parameters and one fitness word per candidate:
+//   * warps 0-7 / 8-15 (epilogue of tile 0 / 1): build the layer-0 input
+//     rows, then per layer read the tile's TMEM accumulator (warp w owns rows
 //     32(w%4).. and column half (w/4)%2), add bias, SiLU, round to BF16 and
 //     write the next layer's A operand in place; after the last layer they
 //     accumulate sum_s |target - mean| / target per row and reduce rows to
 //     candidates in shared memory;
 //   * warp 16 (producer): streams the packed weights, 32 K-columns per stage,
-//     5 stages, with bulk asynchronous copies completing on mbarriers;
+//     5 stages, with bulk asynchronous copies completing on mbarriers; it
+//     runs ahead into the next layer while the epilogue works;
 //   * warp 17 (MMA): one thread issues tcgen05.mma (M = 128, N = layer width,
-//     K = 16), layer by layer alternating between the two slots, so one
-//     slot's epilogue overlaps the other slot's MMAs.
-// TMEM: 512 columns, 256 per slot.
+//     K = 16) for both tiles from every weight stage, so each weight byte
+//     read from L2 serves 256 rows.
+// TMEM: 512 columns, 256 per tile.
 constexpr int SC_BK = 32, SC_STAGES = 5, SC_HID = 256, SC_LAYERS = 5;
-constexpr int SC_EPI = 512;                       // epilogue threads (16 warps)
+constexpr int SC_EPI = 512;                       // epilogue threads (16 warps, 8 per tile)
 constexpr int SC_THREADS = SC_EPI + 64;           // + producer and MMA warps
-constexpr int SC_A_BYTES = 128 * SC_HID * 2;      // one slot's activation tile
+constexpr int SC_A_BYTES = 128 * SC_HID * 2;      // one tile's activations
 constexpr int SC_STAGE_BYTES = SC_HID * SC_BK * 2;
 constexpr int SC_CONST_BYTES = 16384;             // biases, output scaling, target (when it fits)
 
@@ -443,8 +444,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 // Named barrier 1 over the 512 epilogue threads, and the same barrier as a
-// vote: true when every epilogue thread passes true.
+// vote: true when every epilogue thread passes true.  Barrier 2 + tile
+// covers one tile's 256 epilogue threads.
 __device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 512;" ::: "memory"); }
+__device__ __forceinline__ void tile_sync(uint32_t e) { asm volatile("bar.sync %0, 256;" ::"r"(2u + e) : "memory"); }
 __device__ __forceinline__ bool epi_all(bool v) {
     uint32_t r;
     asm volatile(
@@ -469,16 +472,16 @@ __device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// Layer-0 input columns [16 part, 16 part + 16) of row r of the tile:
-// scaled log parameters in [-1, 1], scaled time, zeros (the same FP32
-// operations as surrogate.make_inputs).
-__device__ void sc_build_input(const Screen& p, uint8_t* A, int r, int part, uint32_t row) {
-    float x[16];
-    const int c0 = 16 * part;
+// Layer-0 input columns [32 h, 32 h + 32) of row r of the tile: scaled log
+// parameters in [-1, 1], scaled time, zeros (the same FP32 operations as
+// surrogate.make_inputs).
+__device__ void sc_build_input(const Screen& p, uint8_t* A, int r, int h, uint32_t row) {
+    float x[32];
+    const int c0 = 32 * h;
     const bool live = row < p.n_rows;
     const uint32_t cand = live ? row / p.ns : 0u, ti = live ? row % p.ns : 0u;
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
+    for (int q = 0; q < 32; q++) {
         const int j = c0 + q;
         float v = 0.0f;
         if (live && j < p.n_par) {
@@ -490,7 +493,7 @@ __device__ void sc_build_input(const Screen& p, uint8_t* A, int r, int part, uin
         x[q] = v;
     }
 #pragma unroll
-    for (int kb = 0; kb < 2; kb++) {
+    for (int kb = 0; kb < 4; kb++) {
         uint4 v;
         v.x = pack_bf2(x[kb * 8 + 0], x[kb * 8 + 1]);
         v.y = pack_bf2(x[kb * 8 + 2], x[kb * 8 + 3]);
@@ -508,10 +511,10 @@ __device__ __forceinline__ uint32_t sc_my_tiles(const Screen& p) {
 
 __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(8) uint64_t full[SC_STAGES], empty[SC_STAGES], acc_full[2], a_ready[2], drain;
+    __shared__ __align__(8) uint64_t full[SC_STAGES], empty[SC_STAGES], acc_full, a_ready, drain;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
-    __shared__ float s_acc[132];
+    __shared__ float s_acc[2][132];
     uint8_t* stage = smem + 2 * SC_A_BYTES;
     // per-CTA constants in shared memory: biases [4*256 + out_w], y_mean [S],
     // y_std [S], and the target [ns][S] when it fits
@@ -535,15 +538,13 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], 1);
         }
-        for (int i = 0; i < 2; i++) {
-            mbar_init(&acc_full[i], 1);
-            mbar_init(&a_ready[i], SC_EPI);
-        }
+        mbar_init(&acc_full, 1);
+        mbar_init(&a_ready, SC_EPI);
         mbar_init(&drain, 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = threadIdx.x; i < 132; i += SC_THREADS) s_acc[i] = 0.0f;
+    for (int i = threadIdx.x; i < 2 * 132; i += SC_THREADS) (&s_acc[0][0])[i] = 0.0f;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      ::"r"(smem_u32(&tmem_slot)), "r"(2 * SC_HID));
@@ -555,7 +556,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
     const uint32_t tmem = tmem_slot;
 
     if (warp == 16) {
-        // ---- producer: the weight stream, in the MMA issuer's order ----
+        // ---- producer: the weight stream, once per tile pair and layer ----
         if (lane == 0) {
             uint32_t idx = 0;
             uint32_t issued[SC_STAGES] = {};  // copies issued per stage buffer
@@ -564,17 +565,15 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
                 size_t off = 0;
                 for (int l = 0; l < SC_LAYERS && ok; l++) {
                     const uint32_t bytes = (uint32_t)(sc_n(p, l) * SC_BK * 2);
-                    for (uint32_t i = i0; i < i0 + 2 && i < my && ok; i++) {
-                        for (int ks = 0; ks < sc_k(l) / SC_BK; ks++, idx++) {
-                            const uint32_t sl = idx % SC_STAGES, round = idx / SC_STAGES;
-                            if (round > 0 && !mbar_wait(&empty[sl], (round - 1) & 1u, p.err)) { ok = false; break; }
-                            if (*(volatile int*)&abort_flag) { ok = false; break; }
-                            mbar_expect_tx(&full[sl], bytes);
-                            bulk_g2s(stage + sl * SC_STAGE_BYTES, p.wpack + off + (size_t)ks * bytes, bytes, &full[sl]);
-                            issued[sl]++;
-                        }
+                    for (int ks = 0; ks < sc_k(l) / SC_BK; ks++, idx++) {
+                        const uint32_t sl = idx % SC_STAGES, round = idx / SC_STAGES;
+                        if (round > 0 && !mbar_wait(&empty[sl], (round - 1) & 1u, p.err)) { ok = false; break; }
+                        if (*(volatile int*)&abort_flag) { ok = false; break; }
+                        mbar_expect_tx(&full[sl], bytes);
+                        bulk_g2s(stage + sl * SC_STAGE_BYTES, p.wpack + off, bytes, &full[sl]);
+                        issued[sl]++;
+                        off += bytes;
                     }
-                    off += (size_t)bytes * (sc_k(l) / SC_BK);
                 }
             }
             if (!ok) {
@@ -585,41 +584,36 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
             }
         }
     } else if (warp == 17) {
-        // ---- MMA issuer: per tile pair and layer, slot 0 then slot 1 ----
+        // ---- MMA issuer: every weight stage feeds both tiles ----
         if (lane == 0) {
-            uint32_t idx = 0, nready[2] = {0u, 0u};
+            uint32_t idx = 0, nready = 0;
             bool ok = true;
-            const uint32_t s0 = smem_u32(stage);
+            const uint32_t s0 = smem_u32(stage), a0 = smem_u32(smem), a1 = smem_u32(smem + SC_A_BYTES);
             for (uint32_t i0 = 0; i0 < my && ok; i0 += 2) {
+                const bool two = i0 + 1 < my;
                 for (int l = 0; l < SC_LAYERS && ok; l++) {
+                    if (!mbar_wait(&a_ready, nready & 1u, p.err) || *(volatile int*)&abort_flag) { ok = false; break; }
+                    nready++;
+                    tc_fence_after();
                     const int N = sc_n(p, l);
                     const uint32_t idesc = make_idesc(128, N);
-                    for (uint32_t i = i0; i < i0 + 2 && i < my && ok; i++) {
-                        const uint32_t slot = i & 1u;
-                        if (!mbar_wait(&a_ready[slot], nready[slot] & 1u, p.err) || *(volatile int*)&abort_flag) {
-                            ok = false;
-                            break;
-                        }
-                        nready[slot]++;
+                    for (int ks = 0; ks < sc_k(l) / SC_BK; ks++, idx++) {
+                        const uint32_t sl = idx % SC_STAGES, round = idx / SC_STAGES;
+                        if (!mbar_wait(&full[sl], round & 1u, p.err)) { ok = false; break; }
                         tc_fence_after();
-                        const uint32_t a0 = smem_u32(smem + slot * SC_A_BYTES);
-                        const uint32_t d = tmem + slot * SC_HID;
-                        for (int ks = 0; ks < sc_k(l) / SC_BK; ks++, idx++) {
-                            const uint32_t sl = idx % SC_STAGES, round = idx / SC_STAGES;
-                            if (!mbar_wait(&full[sl], round & 1u, p.err)) { ok = false; break; }
-                            tc_fence_after();
 #pragma unroll
-                            for (int kk = 0; kk < SC_BK / 16; kk++) {
-                                const int k0 = ks * SC_BK + kk * 16;  // K offset in the activation tile
-                                const uint64_t da = make_desc(a0 + (uint32_t)(k0 / 8) * 16u * 128u, 16u * 128u, 128u);
-                                const uint64_t db = make_desc(s0 + sl * SC_STAGE_BYTES + (uint32_t)(kk * 2 * (N / 8) * 128),
-                                                              (uint32_t)((N / 8) * 128), 128u);
-                                mma_bf16(d, da, db, idesc, (ks > 0 || kk > 0) ? 1u : 0u);
-                            }
-                            mma_commit(&empty[sl]);
+                        for (int kk = 0; kk < SC_BK / 16; kk++) {
+                            const int k0 = ks * SC_BK + kk * 16;  // K offset in the activation tiles
+                            const uint32_t ka = (uint32_t)(k0 / 8) * 16u * 128u;
+                            const uint64_t db = make_desc(s0 + sl * SC_STAGE_BYTES + (uint32_t)(kk * 2 * (N / 8) * 128),
+                                                          (uint32_t)((N / 8) * 128), 128u);
+                            const uint32_t acc = (ks > 0 || kk > 0) ? 1u : 0u;
+                            mma_bf16(tmem, make_desc(a0 + ka, 16u * 128u, 128u), db, idesc, acc);
+                            if (two) mma_bf16(tmem + SC_HID, make_desc(a1 + ka, 16u * 128u, 128u), db, idesc, acc);
                         }
-                        if (ok) mma_commit(&acc_full[slot]);
+                        mma_commit(&empty[sl]);
                     }
+                    if (ok) mma_commit(&acc_full);
                 }
             }
             if (!ok) atomicExch(&abort_flag, 1);
@@ -627,51 +621,48 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
             mbar_wait(&drain, 0u, nullptr);
         }
     } else {
-        // ---- epilogue warps 0-15, in the MMA issuer's order (per tile pair
-        // and layer, slot 0 then slot 1): warp w owns rows 32(w%4).. (its TMEM
-        // lane quadrant) and columns [64 part, 64 part + 64), part = w / 4 ----
-        const int q = warp & 3, part = warp >> 2;
+        // ---- epilogue: warps 8e..8e+7 serve tile e; warp w owns rows 32(w%4)..
+        // (its TMEM lane quadrant) and column half h = (w/4)%2 ----
+        const uint32_t e = (uint32_t)warp >> 3;
+        const int q = warp & 3, h = (warp >> 2) & 1;
         const int r = q * 32 + lane;
-        const int et = (int)threadIdx.x;  // 0..511
-        uint32_t nacc[2] = {0u, 0u};
+        const int et = (int)threadIdx.x - (int)e * 256;  // 0..255 within the tile's warps
+        uint8_t* A = smem + e * SC_A_BYTES;
+        float* acc_c = s_acc[e];
+        const uint32_t tbase = tmem + e * SC_HID + ((uint32_t)(q * 32) << 16);
+        uint32_t nacc = 0;
         bool ok = true;
         for (uint32_t i0 = 0; i0 < my && ok; i0 += 2) {
-            for (uint32_t i = i0; i < i0 + 2 && i < my; i++) {  // inputs of the pair's tiles
-                const uint32_t row = (blockIdx.x + i * gridDim.x) * 128u + (uint32_t)r;
-                sc_build_input(p, smem + (i & 1u) * SC_A_BYTES, r, part, row);
-                fence_async_smem();
-                tc_fence_before();
-                mbar_arrive(&a_ready[i & 1u]);
-            }
-            for (int l = 0; l < SC_LAYERS && ok; l++) {
-                for (uint32_t i = i0; i < i0 + 2 && i < my; i++) {
-                    const uint32_t e = i & 1u;
-                    const uint32_t t = blockIdx.x + i * gridDim.x;
-                    const uint32_t row = t * 128u + (uint32_t)r;
-                    uint8_t* A = smem + e * SC_A_BYTES;
-                    const uint32_t tbase = tmem + e * SC_HID + ((uint32_t)(q * 32) << 16);
-                    bool got = mbar_wait(&acc_full[e], nacc[e] & 1u, p.err);
-                    got = epi_all(got && !*(volatile int*)&abort_flag);  // uniform over the epilogue
-                    nacc[e]++;
-                    if (!got) { ok = false; break; }
-                    tc_fence_after();
-                    if (l < SC_LAYERS - 1) {
+            const bool mine = i0 + e < my;  // this pair has a tile for this warp group
+            const uint32_t t = blockIdx.x + (i0 + e) * gridDim.x;
+            const uint32_t row = t * 128u + (uint32_t)r;
+            if (mine) sc_build_input(p, A, r, h, row);
+            fence_async_smem();
+            tc_fence_before();
+            mbar_arrive(&a_ready);
+            for (int l = 0; l < SC_LAYERS; l++) {
+                bool got = mbar_wait(&acc_full, nacc & 1u, p.err);
+                got = epi_all(got && !*(volatile int*)&abort_flag);  // uniform over the epilogue
+                nacc++;
+                if (!got) { ok = false; break; }
+                tc_fence_after();
+                if (l < SC_LAYERS - 1) {
+                    if (mine) {
                         const float* b = c_bias + l * SC_HID;
-                        const int c0 = 64 * part;
+                        const int c0 = 128 * h;
                         uint32_t ra[32], rb[32];
                         tmem_ld32_issue(tbase + (uint32_t)c0, ra);
-                        tmem_wait();
-                        tmem_ld32_issue(tbase + (uint32_t)(c0 + 32), rb);  // in flight during the first chunk
 #pragma unroll
-                        for (int half = 0; half < 2; half++) {
-                            if (half == 1) tmem_wait();
-                            const uint32_t* rr = half == 0 ? ra : rb;
-                            const int c = c0 + 32 * half;
+                        for (int j = 0; j < 4; j++) {  // four 32-column chunks, the next load in flight
+                            tmem_wait();
+                            uint32_t(&cur)[32] = (j & 1) ? rb : ra;
+                            if (j < 3) tmem_ld32_issue(tbase + (uint32_t)(c0 + 32 * (j + 1)), (j & 1) ? ra : rb);
+                            const int c = c0 + 32 * j;
                             const float4* b4 = reinterpret_cast<const float4*>(b + c);
 #pragma unroll
                             for (int k = 0; k < 4; k++) {  // 8 columns -> one 16-byte store
                                 const float4 ba = b4[2 * k], bb = b4[2 * k + 1];
-                                const uint32_t* u = rr + 8 * k;
+                                const uint32_t* u = cur + 8 * k;
                                 uint4 o;
                                 o.x = pack_bf2(silu(__uint_as_float(u[0]) + ba.x), silu(__uint_as_float(u[1]) + ba.y));
                                 o.y = pack_bf2(silu(__uint_as_float(u[2]) + ba.z), silu(__uint_as_float(u[3]) + ba.w));
@@ -680,16 +671,18 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
                                 *reinterpret_cast<uint4*>(A + canon(r, c + 8 * k, 128)) = o;
                             }
                         }
-                        fence_async_smem();
-                        tc_fence_before();
-                        mbar_arrive(&a_ready[e]);
-                    } else {
-                        // fitness terms of this row: sum_s |target - mean| (/ target when
-                        // nonzero), 16-column chunks spread over the four column parts
+                    }
+                    fence_async_smem();
+                    tc_fence_before();
+                    mbar_arrive(&a_ready);
+                } else {
+                    // fitness terms of this row: sum_s |target - mean| (/ target when
+                    // nonzero), 16-column chunks alternating between the column halves
+                    float acc = 0.0f;
+                    if (mine) {
                         const float* b = c_bias + (SC_LAYERS - 1) * SC_HID;
-                        float acc = 0.0f;
                         const uint32_t ti = row % p.ns;
-                        for (int c = 16 * part; c < p.S; c += 64) {
+                        for (int c = 16 * h; c < p.S; c += 32) {
                             float v[16];
                             tmem_ld16(tbase + (uint32_t)c, v);
 #pragma unroll
@@ -704,17 +697,19 @@ __global__ void __launch_bounds__(SC_THREADS, 1) screen_kernel(Screen p) {
                                 }
                             }
                         }
-                        tc_fence_before();
-                        const uint32_t cand0 = (t * 128u) / p.ns;
-                        if (row < p.n_rows && acc != 0.0f) atomicAdd(&s_acc[row / p.ns - cand0], acc);
-                        epi_sync();
-                        const uint32_t last = (min(t * 128u + 127u, p.n_rows - 1u)) / p.ns;
-                        if ((uint32_t)et <= last - cand0 && t * 128u < p.n_rows) {
-                            atomicAdd(&p.fit[cand0 + et], (double)s_acc[et]);
-                            s_acc[et] = 0.0f;
-                        }
-                        epi_sync();
                     }
+                    tc_fence_before();
+                    const uint32_t cand0 = (t * 128u) / p.ns;
+                    if (mine && row < p.n_rows && acc != 0.0f) atomicAdd(&acc_c[row / p.ns - cand0], acc);
+                    tile_sync(e);
+                    if (mine && t * 128u < p.n_rows) {
+                        const uint32_t last = (min(t * 128u + 127u, p.n_rows - 1u)) / p.ns;
+                        if ((uint32_t)et <= last - cand0) {
+                            atomicAdd(&p.fit[cand0 + et], (double)acc_c[et]);
+                            acc_c[et] = 0.0f;
+                        }
+                    }
+                    tile_sync(e);
                 }
             }
         }
