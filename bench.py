@@ -161,7 +161,7 @@ def cpu_reference(net, desc, steps, warmup, sample_s=10.0, threads=None, flags=0
             vals.append(k / dt)
             fvals.append(float(info["firings"].sum()) / dt)
     return float(np.mean(vals)), float(np.mean(fvals)), {
-        "cores": threads, "sample": f"{k} of the {net.n} simulations per step ({desc.split(',')[0]})"}
+        "cores": threads, "k": k, "sample": f"{k} of the {net.n} simulations per step ({desc.split(',')[0]})"}
 
 
 def cpu_reference_segments(segs, steps, warmup, flags=0):
@@ -169,14 +169,16 @@ def cpu_reference_segments(segs, steps, warmup, flags=0):
     sum of per-segment times (each measured on a bounded sample)."""
     tot_n, tot_t, tot_f, meta = 0, 0.0, 0.0, None
     budget = 10.0 / len(segs)
-    samples = []
+    samples, sample_ms = [], 0.0
     for net, desc in segs:
         v, fv, meta = cpu_reference(net, desc, steps, warmup, sample_s=budget, flags=flags)
         tot_n += net.n
         tot_t += net.n / v
         tot_f += fv * (net.n / v)
         samples.append(meta["sample"])
-    return tot_n / tot_t, tot_f / tot_t, {"cores": meta["cores"], "sample": "; ".join(samples)}
+        sample_ms += 1e3 * meta["k"] / v
+    return tot_n / tot_t, tot_f / tot_t, {"cores": meta["cores"], "sample": "; ".join(samples),
+                                          "sample_ms": sample_ms}
 
 
 def measured_peaks():
@@ -357,7 +359,8 @@ def main():
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": "sims/s",
             "firings_per_s": fv, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": meta["sample_ms"], "ms_per_step_is": "one bounded sample step (see cpu_baseline.sample)",
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32/f64/i32", "data": "synthetic",
             "config": {"workload": desc, "sims": n_total},
             "cpu_baseline": {"value": v, "unit": "sims/s", "cores": meta["cores"], "kind": "port",
