@@ -271,7 +271,8 @@ def bench_config5(a):
     level = truth * 1.02
 
     def run_until(mode, offset, **kw):
-        hist = fs.cem(p, mode=mode, generations=max_gen, pop=pop, seed=1, stop_at=level, **kw)
+        hist = fs.cem(p, mode=mode, generations=max_gen, pop=pop, seed=1, stop_at=level,
+                      time_limit=a.time_limit, **kw)
         reached = hist[-1][2] <= level
         return offset + hist[-1][0], hist[-1][1], reached, hist
     torch.cuda.synchronize()
@@ -293,7 +294,8 @@ def bench_config5(a):
                                      "n_rep": n_rep, "training_trajectories": n_traj, "screened_per_gen": screen,
                                      "surrogate_iterations_per_gen": a.inner,
                                      "finetune_steps_per_gen": a.finetune,
-                                     "resimulated_per_gen": pop, "max_generations": max_gen},
+                                     "resimulated_per_gen": pop, "max_generations": max_gen,
+                                     "time_limit_s": a.time_limit},
         "roofline": scr, "gpu_launches": None,
         "value": 1.0 / ts, "unit": "fits/s (surrogate-screened)", "plain_fits_per_s": 1.0 / tp,
         "speedup_vs_plain": tp / ts, "speedup_is_lower_bound": not plain_ok, "surrogate_reached": surr_ok,
@@ -317,6 +319,8 @@ def main():
     ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5])
     ap.add_argument("--full", action="store_true", help="config 5 at the configured sizes")
     ap.add_argument("--inner", type=int, default=1, help="config 5: surrogate-only iterations per generation")
+    ap.add_argument("--time-limit", type=float, default=None,
+                    help="config 5: wall-second cap per search (a capped plain search makes the speed-up a lower bound)")
     ap.add_argument("--screen-only", action="store_true", help="config 5: time the fused screening kernel alone")
     ap.add_argument("--finetune", type=int, default=100,
                     help="config 5: surrogate fine-tuning steps per generation on the re-simulated trajectories")
