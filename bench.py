@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--config 2]
 
-Workload (default): the synthetic mass-action network of configs[1] -- 64
+Workload (default, config 2): the synthetic mass-action network -- 64
 species, 128 reactions of order 0-2 (generator seed 0), rate constants
 log-uniform in [1e-4, 1], initial counts log-uniform in [10, 1e4] -- for
 65,536 simulations per GPU, t_end = 10, 200 samples, eps = 0.03.  One step =

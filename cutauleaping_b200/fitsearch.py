@@ -13,7 +13,7 @@ log-parameter space:
 * surrogate: every generation screens many candidates with the MLP
              surrogate (cutauleaping_b200.surrogate), re-simulates only the
              best 1% with the plain method and keeps the elite by that true
-             fitness; the plain method is the fallback and the judge.
+             fitness; the plain method is the fallback and the arbiter.
 
 All simulation goes through the CUDA sweep (ctl_run_device) and the fitness
 through calculateFitness on the device (ctl_fitness_device).

@@ -4,7 +4,7 @@ The reference computes the fitness of every candidate parameter set by full
 simulation (kernel.cu:365-423, calculateFitness 2phase_n-tau-leaping.cu:
 3324-3408).  Here a small MLP, trained on trajectories the simulator itself
 produces, screens candidates first; every retained candidate is re-simulated
-with the plain method, which also judges the surrogate's error.
+with the plain method, which also measures the surrogate's error.
 
 Network: x = (8 scaled log rate constants, scaled t) -> 256 -> 256 -> 256 ->
 256 -> 2*S (per-species mean and log-variance of the standardised counts),
