@@ -12,7 +12,14 @@ reference's own trajectories (3-standard-error and two-sample KS checks).
 
 Run on a machine with a GPU (the reference has no CPU path):
     python tests/golden/make_reference_fixtures.py --out tests/golden
+
+With --time it instead times the reference binary on the Schlogl benchmark
+workload (4,096 simulations, t_end 5, 100 samples, 64 threads x 64 blocks):
+the reference's own timer around its simulation loop (" * RUNNING TIME",
+kernel.cu:240-347, printed with verbose = 1; file output comes after it),
+three runs, printed as one JSON line.
 """
+import json
 import argparse
 import os
 import subprocess
@@ -100,14 +107,40 @@ def run_case(name, factory, threads, blocks, force, keep, outdir):
     print(f"{name}: {n} simulations, reference wall {wall:.2f}s -> {path}", flush=True)
 
 
+def time_reference(runs=3):
+    """Seconds of the reference's own simulation-loop timer on the Schlogl
+    benchmark workload, per run."""
+    net = inputs.schlogl(4096)
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        folder = inputs.write_folder(os.path.join(td, "schlogl"), net)
+        for i in range(runs):
+            out = os.path.join(td, f"out{i}")
+            args = [REF_BIN, folder, "64", "64", "0", "0", out, "pref", "0", "0", "1"]
+            p = subprocess.run(args, capture_output=True, text=True, timeout=900)
+            if p.returncode != 0:
+                raise RuntimeError(f"reference exited {p.returncode}: {p.stderr[-2000:]}")
+            t = [float(l.split(":")[1].split()[0]) for l in p.stdout.splitlines() if "RUNNING TIME" in l]
+            if not t:
+                raise RuntimeError("no RUNNING TIME line in the reference's output")
+            times.append(t[-1])
+    return times
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
     ap.add_argument("--cases", nargs="*", default=list(CASES))
+    ap.add_argument("--time", action="store_true", help="time the reference binary on the Schlogl workload")
     a = ap.parse_args()
-    os.makedirs(a.out, exist_ok=True)
     if not os.path.exists(REF_BIN):
         sys.exit(f"{REF_BIN} missing: build it with `make -C oracle ref` where the reference sources exist")
+    if a.time:
+        t = time_reference()
+        print(json.dumps({"workload": "Schlogl, 4096 simulations, t_end 5, 100 samples, 64 threads x 64 blocks",
+                          "reference_running_time_s": t, "sims_per_s_best": 4096 / min(t)}), flush=True)
+        return
+    os.makedirs(a.out, exist_ok=True)
     for name in a.cases:
         run_case(name, *CASES[name], a.out)
 
