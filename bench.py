@@ -440,8 +440,16 @@ def main():
         fire += float(inf["firings"].sum())
         ops += op_count(pt["net"], inf)
         abytes += algorithmic_bytes(pt["net"]) * pt["net"].n
-        per_sim[pt["net"].name] = {"steps": float(inf["steps"].mean()), "leaps": float(inf["leaps"].mean()),
+        steps = inf["steps"].astype(np.float64)
+        # step histogram: how simulations split between leap- and SSA-dominated regimes
+        leap_share = inf["leaps"] / np.maximum(inf["leaps"] + inf["ssa_steps"], 1)
+        per_sim[pt["net"].name] = {"steps": float(steps.mean()), "leaps": float(inf["leaps"].mean()),
                                    "ssa_steps": float(inf["ssa_steps"].mean()),
+                                   "steps_quantiles": {q: float(np.percentile(steps, v)) for q, v in
+                                                       (("p10", 10), ("p50", 50), ("p90", 90), ("p99", 99),
+                                                        ("max", 100))},
+                                   "leap_share_histogram": np.histogram(leap_share, bins=10,
+                                                                        range=(0.0, 1.0))[0].tolist(),
                                    "status_ok": int((inf["status"] == 0).sum())}
     if dist is not None:
         f = torch.tensor([fire], dtype=torch.float64, device=dev)
