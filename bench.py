@@ -252,8 +252,10 @@ def bench_config5(a):
     parameters (the attainable floor at this replicate count), or a generation
     cap.  The surrogate search pays for its training data and training inside
     its wall time, and after every generation fine-tunes the network on 8 of
-    the trajectories it just simulated per candidate (so its error shrinks
-    where the search is).  fits/s = 1 / wall seconds to reach that level;
+    the trajectories it just simulated per candidate for half of them (half
+    of each batch replayed from the original training data), keeping the
+    fine-tuned weights only if the surrogate's error on the other half's
+    simulated fitness went down.  fits/s = 1 / wall seconds to reach that level;
     when plain search does not reach it within the cap, the speed-up is a
     lower bound.  Reduced size (default): 256 replicates, 2^16 training
     trajectories, 1e5 screened and 1,000 re-simulated per generation; --full:
@@ -284,8 +286,9 @@ def bench_config5(a):
     net, sc = fs.train_surrogate(p, theta, traj, epochs=2, batch=16384)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0 - t_data
+    ft_log = []
     ts, ss, surr_ok, sh = run_until("surrogate", t_data + t_train, screen=screen, keep_frac=0.01, net=net, sc=sc,
-                                    inner=a.inner, finetune_steps=a.finetune)
+                                    inner=a.inner, finetune_steps=a.finetune, replay=(theta, traj), log=ft_log)
     scr = screen_roofline(p, net, sc, n_cand=200_000)
     print(json.dumps({
         "metric": METRIC, "config": {"workload": "surrogate-screened parameter estimation: 32x64 network "
@@ -304,6 +307,9 @@ def bench_config5(a):
         "time_s": {"plain_to_level": tp, "surrogate_to_level": ts, "surrogate_data": t_data,
                    "surrogate_training": t_train},
         "generations": {"plain": len(ph), "surrogate": len(sh)},
+        "finetune": {"phases": len(ft_log), "kept": sum(1 for x in ft_log if x["kept"]),
+                     "surrogate_error": [[round(x["surrogate_error_before"], 4), round(x["after"], 4)]
+                                         for x in ft_log]},
         "simulations_to_level": {"plain": sp, "surrogate": ss},
         "curves": {"plain": [[round(h[0], 3), h[2]] for h in ph],
                    "surrogate": [[round(h[0] + t_data + t_train, 3), h[2]] for h in sh]},

@@ -146,17 +146,22 @@ def training_data(p: FitProblem, n_traj, *, seed=5, sim_seed=91):
 
 
 def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-3, seed=0, log=None,
-                    net=None, sc=None, steps=None, cosine=True):
+                    net=None, sc=None, steps=None, cosine=True, replay=None):
     """Fit the MLP to (theta, t) -> counts of single trajectories (Gaussian
     NLL: the network learns the ensemble mean and log-variance).  With `net`
     and `sc` given, continues training that network (fine-tuning) with its
-    output scaling unchanged."""
+    output scaling unchanged; with `replay` = (theta0, traj0), half of every
+    batch is drawn from that earlier data so the network keeps what it knew
+    outside the new data's region."""
     import torch
     n, ns, S = traj.shape
-    y = traj.to(torch.float32)
     if sc is None:
-        y_mean = y.mean(dim=(0, 1))
-        y_std = y.std(dim=(0, 1)).clamp_min(1.0)
+        # per-species scale from a sample of the trajectories
+        ix = torch.randint(0, n, (min(n, 1 << 14),), device="cuda",
+                           generator=torch.Generator(device="cuda").manual_seed(seed))
+        ys = traj[ix].to(torch.float32)
+        y_mean = ys.mean(dim=(0, 1))
+        y_std = ys.std(dim=(0, 1)).clamp_min(1.0)
         sc = sg.Scaling(p.log_lo, p.log_hi, float(p.tvec[-1]), y_mean.cpu().numpy(), y_std.cpu().numpy())
     else:
         y_mean = torch.as_tensor(sc.y_mean, dtype=torch.float32, device="cuda")
@@ -166,13 +171,20 @@ def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-
         net = sg.MLP(S, seed=seed)
     total = n * ns
     steps = steps or max(1, (epochs * total) // batch)
-    g = torch.Generator(device="cuda").manual_seed(seed + net.step_count)
+    g = torch.Generator(device="cuda").manual_seed(seed + net.version)
+    sources = [(theta, traj, batch if replay is None else batch // 2)]
+    if replay is not None:
+        sources.append((replay[0], replay[1], batch - batch // 2))
     hist = []
     for it in range(steps):
-        idx = torch.randint(0, total, (batch,), device="cuda", generator=g)
-        si, ti = idx // ns, idx % ns
-        X = sg.make_inputs(theta[si], tv[ti], sc, torch)
-        tgt = (y[si, ti] - y_mean) / y_std
+        Xs, Ts = [], []
+        for th_, tr_, k in sources:
+            idx = torch.randint(0, tr_.shape[0] * ns, (k,), device="cuda", generator=g)
+            si, ti = idx // ns, idx % ns
+            Xs.append(sg.make_inputs(th_[si], tv[ti], sc, torch))
+            Ts.append((tr_[si, ti].to(torch.float32) - y_mean) / y_std)
+        X = Xs[0] if len(Xs) == 1 else torch.cat(Xs)
+        tgt = Ts[0] if len(Ts) == 1 else torch.cat(Ts)
         out = net.forward(X)
         loss, dW, db = net.backward(out, tgt)
         rate = lr * 0.5 * (1 + math.cos(math.pi * it / steps)) if cosine else lr
@@ -226,9 +238,15 @@ def predicted_fitness_layers(p: FitProblem, net, sc, theta_log, *, chunk=65536):
 # Cross-entropy search
 # ---------------------------------------------------------------------------
 
+def _surrogate_error(p, net, sc, cand, f):
+    """Mean relative error of the surrogate's fitness against simulated fitness."""
+    pf = predicted_fitness(p, net, sc, cand)
+    return float(np.mean(np.abs(pf - f) / np.maximum(f, 1e-12)))
+
+
 def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_frac=0.01, net=None,
         sc=None, seed=0, sim_seed=1000, time_limit=None, stop_at=None, inner=1, explore_frac=0.0,
-        finetune_steps=0, finetune_reps=8, finetune_lr=5e-4, finetune_batch=8192):
+        finetune_steps=0, finetune_reps=8, finetune_lr=2e-4, finetune_batch=8192, replay=None, log=None):
     """Cross-entropy search in log-parameter space.
 
     mode 'plain' simulates every one of `pop` candidates per generation.
@@ -238,12 +256,17 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
     fitness; the last one keeps its screened set), then re-simulates the best
     max(pop, keep_frac * screen) screened candidates -- of which a fraction
     `explore_frac` is replaced by unscreened draws from the proposal -- and
-    refits the proposal to their best by true fitness.  With
-    finetune_steps > 0 the surrogate is then fine-tuned on `finetune_reps`
-    of the trajectories just simulated per candidate, so its error shrinks
-    where the search is.  Every candidate whose fitness is reported was
-    simulated.  Returns a list of (wall seconds, simulations so far, best
-    true fitness, best theta), one entry per generation."""
+    refits the proposal to their best by true fitness.
+
+    With finetune_steps > 0 the surrogate is then fine-tuned on
+    `finetune_reps` of the trajectories just simulated for half of those
+    candidates (fresh optimiser moments, constant rate, half of every batch
+    replayed from `replay` = the original training data when given), and the
+    simulated fitness of the other half judges the result: the fine-tuned
+    weights are kept only if the surrogate's error on that half went down.
+    Every candidate whose fitness is reported was simulated.  Returns a list
+    of (wall seconds, simulations so far, best true fitness, best theta), one
+    entry per generation; `log`, if a list, receives per-generation notes."""
     import torch
     rng = np.random.default_rng(seed)
     d = len(p.unknown)
@@ -288,8 +311,19 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
         if stop_at is not None and best_f <= stop_at:
             break
         if mode != "plain" and finetune_steps:
-            th = torch.as_tensor(np.repeat(cand, min(finetune_reps, p.n_rep), axis=0), dtype=torch.float32,
-                                 device="cuda")
-            train_surrogate(p, th, traj, net=net, sc=sc, steps=finetune_steps, lr=finetune_lr,
-                            batch=finetune_batch, cosine=False)
+            reps = min(finetune_reps, p.n_rep)
+            tr_idx, va_idx = np.arange(0, len(cand), 2), np.arange(1, len(cand), 2)
+            before = _surrogate_error(p, net, sc, cand[va_idx], f[va_idx])
+            saved = net.state()
+            net.reset_optimizer()
+            rows = torch.as_tensor((tr_idx[:, None] * reps + np.arange(reps)[None, :]).reshape(-1), device="cuda")
+            th = torch.as_tensor(np.repeat(cand[tr_idx], reps, axis=0), dtype=torch.float32, device="cuda")
+            train_surrogate(p, th, traj[rows], net=net, sc=sc, steps=finetune_steps, lr=finetune_lr,
+                            batch=finetune_batch, cosine=False, replay=replay)
+            after = _surrogate_error(p, net, sc, cand[va_idx], f[va_idx])
+            kept = after < before
+            if not kept:
+                net.load_state(saved)
+            if log is not None:
+                log.append({"gen": gen, "surrogate_error_before": before, "after": after, "kept": bool(kept)})
     return hist

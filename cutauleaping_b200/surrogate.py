@@ -141,7 +141,8 @@ class MLP:
             self.v.append(torch.zeros_like(w))
             self.mb.append(torch.zeros(fan_out, device="cuda"))
             self.vb.append(torch.zeros(fan_out, device="cuda"))
-        self.step_count = 0
+        self.step_count = 0   # Adam's bias-correction step
+        self.version = 0      # changes with every weight update (keys the packed copy)
         self.err = torch.zeros(1, dtype=torch.int32, device="cuda")
         self._bufs = {}
 
@@ -214,6 +215,7 @@ class MLP:
     def adam(self, dW, db, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, wd=0.0):
         L = _bind()
         self.step_count += 1
+        self.version += 1
         for l in range(len(self.W)):
             rows, cols = self.W[l].shape
             st = L.ctl_mlp_adam(_ptr(self.W[l]), _ptr(dW[l]), _ptr(self.m[l]), _ptr(self.v[l]), rows, cols,
@@ -230,7 +232,7 @@ class MLP:
         """Weights in the screening kernel's streaming layout and the
         concatenated biases; rebuilt after every Adam step."""
         torch = self.torch
-        if getattr(self, "_packed_at", None) != self.step_count:
+        if getattr(self, "_packed_at", None) != self.version:
             L = _bind()
             wp = torch.empty(L.ctl_mlp_pack_bytes(self.out_w) // 2, dtype=torch.bfloat16, device="cuda")
             ptrs = (C.c_void_p * 5)(*[w.data_ptr() for w in self.Wb])
@@ -240,8 +242,31 @@ class MLP:
                 raise CtlError(st, "ctl_mlp_pack")
             self._wpack = wp
             self._bias = torch.cat(self.b).contiguous()
-            self._packed_at = self.step_count
+            self._packed_at = self.version
         return self._wpack, self._bias
+
+    # -- optimiser state ---------------------------------------------------------
+    _STATE = ("W", "b", "Wb", "WbT", "m", "v", "mb", "vb")
+
+    def state(self):
+        """A copy of the weights and the optimiser state."""
+        st = {k: [t.clone() for t in getattr(self, k)] for k in self._STATE}
+        st["step_count"] = self.step_count
+        return st
+
+    def load_state(self, st):
+        for k in self._STATE:
+            for dst, src in zip(getattr(self, k), st[k]):
+                dst.copy_(src)
+        self.step_count = st["step_count"]
+        self.version += 1
+
+    def reset_optimizer(self):
+        """Fresh Adam moments (and bias correction) for a new training phase."""
+        for k in ("m", "v", "mb", "vb"):
+            for t in getattr(self, k):
+                t.zero_()
+        self.step_count = 0
 
     def check_error_flag(self):
         if int(self.err.item()) != 0:

@@ -69,3 +69,27 @@ def test_search_runs_and_records_budget(trained, inner):
                   inner=inner)
     assert surr[-1][1] == plain[-1][1] == 2 * 64 * p.n_rep   # equal simulation budgets
     assert all(h[2] <= g[2] for g, h in zip(surr, surr[1:]))  # best fitness never worsens
+
+
+def test_guarded_finetuning_keeps_or_restores(trained):
+    """Fine-tuning on re-simulated trajectories is judged by simulated
+    fitness on held-out candidates: the log says whether the new weights were
+    kept, and a rejected phase leaves the surrogate's predictions unchanged."""
+    import torch
+    from cutauleaping_b200 import fitsearch as fs
+    p, net, sc, _ = trained
+    theta, traj = fs.training_data(p, 1 << 12, seed=9)
+    probe = np.random.default_rng(5).uniform(p.log_lo, p.log_hi, size=(64, len(p.unknown)))
+    log = []
+    before = net.state()
+    fs.cem(p, mode="surrogate", generations=2, pop=64, screen=6400, keep_frac=0.01, net=net, sc=sc, seed=3,
+           finetune_steps=20, replay=(theta, traj), log=log)
+    assert len(log) == 2 and all(set(x) >= {"surrogate_error_before", "after", "kept"} for x in log)
+    net.check_error_flag()
+    pf_now = fs.predicted_fitness(p, net, sc, probe)
+    assert np.isfinite(pf_now).all()
+    if not any(x["kept"] for x in log):
+        net2_pf = pf_now
+        net.load_state(before)
+        assert np.array_equal(fs.predicted_fitness(p, net, sc, probe), net2_pf)
+    net.load_state(before)  # leave the module fixture as it was
