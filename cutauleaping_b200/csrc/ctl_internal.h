@@ -44,6 +44,16 @@ struct DeviceCopy {
     size_t off_reac_desc = 0;
 };
 
+// Shifts of the stored levels of the propensity sum tree over P = 2^logP
+// leaves: 3, 6, 9, ... below logP, then logP (the root).  Stored level li
+// holds the nodes that cover 2^shift leaves.
+inline int stored_level_shifts(int logP, int (&shift)[10]) {
+    int n = 0;
+    for (int l = 3; l < logP; l += 3) shift[n++] = l;
+    shift[n++] = logP;
+    return n;
+}
+
 void set_error(const std::string& msg);
 ctl_status build_tables(int S, int R, const int32_t* left, const int32_t* right,
                         const int32_t* feed, int ns, const double* tvec, int s_out,

@@ -112,6 +112,48 @@ static ctl_status cuda_fail(cudaError_t e, const char* what) {
 
 static size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
+// The model tables in one device buffer: offsets of every array (`place`
+// returns the next 16-byte aligned offset) and the copy of its contents
+// (`put` returns false to stop); shared by the cached per-device copy and the
+// allocation-free path.
+template <class Place>
+static void table_layout(const HostTables& t, DeviceCopy& d, Place&& place) {
+    d.off_reac_off = place(t.reac_off.size() * 4);
+    d.off_reac_ent = place(std::max<size_t>(1, t.reac_ent.size()) * 4);
+    d.off_reac_desc = place(t.reac_desc.size() * 4);
+    d.off_vs_off = place(t.vs_off.size() * 4);
+    d.off_vs_ent = place(std::max<size_t>(1, t.vs_ent.size()) * 4);
+    d.off_fs_off = place(t.fs_off.size() * 4);
+    d.off_fs_ent = place(std::max<size_t>(1, t.fs_ent.size()) * 4);
+    d.off_fr_off = place(t.fr_off.size() * 4);
+    d.off_fr_ent = place(std::max<size_t>(1, t.fr_ent.size()) * 4);
+    d.off_dep_off = place(t.dep_off.size() * 4);
+    d.off_dep_ent = place(std::max<size_t>(1, t.dep_ent.size()) * 4);
+    d.off_hor = place(t.hor.size());
+    d.off_hort = place(t.hort.size());
+    d.off_tvec = place(t.tvec.size() * 8);
+    d.off_cs = place(t.cs.size() * 4);
+}
+
+template <class Put>
+static void table_fill(const HostTables& t, const DeviceCopy& d, Put&& put) {
+    put(d.off_reac_off, t.reac_off.data(), t.reac_off.size() * 4) &&
+        put(d.off_reac_ent, t.reac_ent.data(), t.reac_ent.size() * 4) &&
+        put(d.off_reac_desc, t.reac_desc.data(), t.reac_desc.size() * 4) &&
+        put(d.off_vs_off, t.vs_off.data(), t.vs_off.size() * 4) &&
+        put(d.off_vs_ent, t.vs_ent.data(), t.vs_ent.size() * 4) &&
+        put(d.off_fs_off, t.fs_off.data(), t.fs_off.size() * 4) &&
+        put(d.off_fs_ent, t.fs_ent.data(), t.fs_ent.size() * 4) &&
+        put(d.off_fr_off, t.fr_off.data(), t.fr_off.size() * 4) &&
+        put(d.off_fr_ent, t.fr_ent.data(), t.fr_ent.size() * 4) &&
+        put(d.off_dep_off, t.dep_off.data(), t.dep_off.size() * 4) &&
+        put(d.off_dep_ent, t.dep_ent.data(), t.dep_ent.size() * 4) &&
+        put(d.off_hor, t.hor.data(), t.hor.size()) &&
+        put(d.off_hort, t.hort.data(), t.hort.size()) &&
+        put(d.off_tvec, t.tvec.data(), t.tvec.size() * 8) &&
+        put(d.off_cs, t.cs.data(), t.cs.size() * 4);
+}
+
 // Upload the model tables to `device` once; later runs reuse them.
 static ctl_status ensure_device(ctl_model* m, int device, DeviceCopy*& out) {
     if (device < 0 || device >= 16) {
@@ -131,42 +173,17 @@ static ctl_status ensure_device(ctl_model* m, int device, DeviceCopy*& out) {
         off = align16(off + bytes);
         return o;
     };
-    d.off_reac_off = place(t.reac_off.size() * 4);
-    d.off_reac_ent = place(std::max<size_t>(1, t.reac_ent.size()) * 4);
-    d.off_reac_desc = place(t.reac_desc.size() * 4);
-    d.off_vs_off = place(t.vs_off.size() * 4);
-    d.off_vs_ent = place(std::max<size_t>(1, t.vs_ent.size()) * 4);
-    d.off_fs_off = place(t.fs_off.size() * 4);
-    d.off_fs_ent = place(std::max<size_t>(1, t.fs_ent.size()) * 4);
-    d.off_fr_off = place(t.fr_off.size() * 4);
-    d.off_fr_ent = place(std::max<size_t>(1, t.fr_ent.size()) * 4);
-    d.off_dep_off = place(t.dep_off.size() * 4);
-    d.off_dep_ent = place(std::max<size_t>(1, t.dep_ent.size()) * 4);
-    d.off_hor = place(t.hor.size());
-    d.off_hort = place(t.hort.size());
-    d.off_tvec = place(t.tvec.size() * 8);
-    d.off_cs = place(t.cs.size() * 4);
+    table_layout(t, d, place);
     size_t ctrl_off = place(256);
     d.bytes = off;
     std::vector<unsigned char> h(d.bytes, 0);
     auto put = [&](size_t o, const void* p, size_t bytes) {
         if (bytes) std::memcpy(h.data() + o, p, bytes);
     };
-    put(d.off_reac_off, t.reac_off.data(), t.reac_off.size() * 4);
-    put(d.off_reac_ent, t.reac_ent.data(), t.reac_ent.size() * 4);
-    put(d.off_reac_desc, t.reac_desc.data(), t.reac_desc.size() * 4);
-    put(d.off_vs_off, t.vs_off.data(), t.vs_off.size() * 4);
-    put(d.off_vs_ent, t.vs_ent.data(), t.vs_ent.size() * 4);
-    put(d.off_fs_off, t.fs_off.data(), t.fs_off.size() * 4);
-    put(d.off_fs_ent, t.fs_ent.data(), t.fs_ent.size() * 4);
-    put(d.off_fr_off, t.fr_off.data(), t.fr_off.size() * 4);
-    put(d.off_fr_ent, t.fr_ent.data(), t.fr_ent.size() * 4);
-    put(d.off_dep_off, t.dep_off.data(), t.dep_off.size() * 4);
-    put(d.off_dep_ent, t.dep_ent.data(), t.dep_ent.size() * 4);
-    put(d.off_hor, t.hor.data(), t.hor.size());
-    put(d.off_hort, t.hort.data(), t.hort.size());
-    put(d.off_tvec, t.tvec.data(), t.tvec.size() * 8);
-    put(d.off_cs, t.cs.data(), t.cs.size() * 4);
+    table_fill(t, d, [&](size_t o, const void* p, size_t bytes) {
+        put(o, p, bytes);
+        return true;
+    });
     int prev = 0;
     CTL_CUDA(cudaGetDevice(&prev));
     CTL_CUDA(cudaSetDevice(device));
@@ -228,22 +245,18 @@ struct LaunchPlan {
 // Stored levels of the sum tree for P = 2^k leaves: 3, 6, ... below k, then
 // k (the root).  Level li is the pairwise sum of 2^d nodes of level li-1.
 static void tree_levels(const HostTables& t, dev::Model& dm) {
-    const int k = t.logP;
-    int prev = 0, base = 0, n = 0;
-    for (int l = 3; l < k; l += 3) {
-        dm.lev_shift[n] = l;
-        dm.lev_d[n] = l - prev;
-        dm.lev_base[n] = base;
-        dm.lev_count[n] = t.P >> l;
-        base += t.P >> l;
-        prev = l;
-        n++;
+    int shift[10];
+    const int nlev = stored_level_shifts(t.logP, shift);
+    int prev = 0, base = 0;
+    for (int li = 0; li < nlev; li++) {
+        dm.lev_shift[li] = shift[li];
+        dm.lev_d[li] = shift[li] - prev;
+        dm.lev_base[li] = base;
+        dm.lev_count[li] = t.P >> shift[li];
+        base += t.P >> shift[li];
+        prev = shift[li];
     }
-    dm.lev_shift[n] = k;
-    dm.lev_d[n] = k - prev;
-    dm.lev_base[n] = base;
-    dm.lev_count[n] = 1;
-    dm.nlev = n + 1;
+    dm.nlev = nlev;
 }
 
 static int tree_words(const HostTables& t) {
@@ -1159,21 +1172,7 @@ extern "C" ctl_status ctl_run_device_noalloc(ctl_model* m, const ctl_run_cfg* cf
         off = align16(off + bytes);
         return o;
     };
-    d.off_reac_off = place(t.reac_off.size() * 4);
-    d.off_reac_ent = place(std::max<size_t>(1, t.reac_ent.size()) * 4);
-    d.off_reac_desc = place(t.reac_desc.size() * 4);
-    d.off_vs_off = place(t.vs_off.size() * 4);
-    d.off_vs_ent = place(std::max<size_t>(1, t.vs_ent.size()) * 4);
-    d.off_fs_off = place(t.fs_off.size() * 4);
-    d.off_fs_ent = place(std::max<size_t>(1, t.fs_ent.size()) * 4);
-    d.off_fr_off = place(t.fr_off.size() * 4);
-    d.off_fr_ent = place(std::max<size_t>(1, t.fr_ent.size()) * 4);
-    d.off_dep_off = place(t.dep_off.size() * 4);
-    d.off_dep_ent = place(std::max<size_t>(1, t.dep_ent.size()) * 4);
-    d.off_hor = place(t.hor.size());
-    d.off_hort = place(t.hort.size());
-    d.off_tvec = place(t.tvec.size() * 8);
-    d.off_cs = place(t.cs.size() * 4);
+    table_layout(t, d, place);
     if (off > NOALLOC_BYTES) {
         set_error("ctl_run_device_noalloc: the model tables need " + std::to_string(off) +
                   " bytes, the allocation-free path holds at most " + std::to_string(NOALLOC_BYTES) +
@@ -1209,21 +1208,10 @@ extern "C" ctl_status ctl_run_device_noalloc(ctl_model* m, const ctl_run_cfg* cf
         return bytes ? cudaMemcpyAsync(b + o, src, bytes, cudaMemcpyHostToDevice, s) : cudaSuccess;
     };
     cudaError_t e = cudaSuccess;
-    if (e == cudaSuccess) e = put(d.off_reac_off, t.reac_off.data(), t.reac_off.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_reac_ent, t.reac_ent.data(), t.reac_ent.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_reac_desc, t.reac_desc.data(), t.reac_desc.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_vs_off, t.vs_off.data(), t.vs_off.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_vs_ent, t.vs_ent.data(), t.vs_ent.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_fs_off, t.fs_off.data(), t.fs_off.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_fs_ent, t.fs_ent.data(), t.fs_ent.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_fr_off, t.fr_off.data(), t.fr_off.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_fr_ent, t.fr_ent.data(), t.fr_ent.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_dep_off, t.dep_off.data(), t.dep_off.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_dep_ent, t.dep_ent.data(), t.dep_ent.size() * 4);
-    if (e == cudaSuccess) e = put(d.off_hor, t.hor.data(), t.hor.size());
-    if (e == cudaSuccess) e = put(d.off_hort, t.hort.data(), t.hort.size());
-    if (e == cudaSuccess) e = put(d.off_tvec, t.tvec.data(), t.tvec.size() * 8);
-    if (e == cudaSuccess) e = put(d.off_cs, t.cs.data(), t.cs.size() * 4);
+    table_fill(t, d, [&](size_t o, const void* src, size_t bytes) {
+        e = put(o, src, bytes);
+        return e == cudaSuccess;
+    });
     if (e != cudaSuccess) return cuda_fail(e, "ctl_run_device_noalloc (tables)");
     LaunchPlan pl;
     if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;

@@ -701,9 +701,12 @@ __device__ int decide_step(const Grp<G>& g, const Model& m, const Run& run, cons
         uint8_t cr = 0;
         const uint32_t e1 = m.reac_off[r + 1];
         for (uint32_t e = m.reac_off[r]; e < e1; e++) {
+            // floor(x / L) < n_c  <=>  x < n_c * L, and floor(x / L) > 0  <=>  x >= L
+            // (x >= 0, L >= 1): the reference's integer test without a division
             const uint32_t ent = m.reac_ent[e];
-            const uint32_t q = (uint32_t)sl.x((int)(ent >> 8)) / (ent & 0xffu);
-            if ((fl & F_Q6_OFF) ? (q < run.nc) : (q > 0u && q < run.nc)) cr = 1;
+            const uint32_t x = (uint32_t)sl.x((int)(ent >> 8)), L = ent & 0xffu;
+            const bool below = (uint64_t)x < (uint64_t)run.nc * L;
+            if ((fl & F_Q6_OFF) ? below : (x >= L && below)) cr = 1;
         }
         sl.cr(r) = cr;
         lany |= cr != 0;
