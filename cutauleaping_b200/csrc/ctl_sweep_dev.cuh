@@ -696,20 +696,29 @@ __device__ int decide_step(const Grp<G>& g, const Model& m, const Run& run, cons
         st.T = m.tmax + (double)0.1f;
         return DONE;
     }
+    // Critical reactions (tau.cu:1727-1733): some reactant with
+    // 0 < floor(x / L) < n_c.  floor(x / L) < n_c  <=>  x < n_c * L and
+    // floor(x / L) > 0  <=>  x >= L (x >= 0, L >= 1): the reference's integer
+    // test without a division.  Reactions with at most two reactant entries
+    // read their packed descriptor (one load), the rest their list.
+    const bool q6off = (fl & F_Q6_OFF) != 0;
+    auto crit_entry = [&](uint32_t ent) {
+        const uint32_t x = (uint32_t)sl.x((int)(ent >> 8)), L = ent & 0xffu;
+        const bool below = (uint64_t)x < (uint64_t)run.nc * L;
+        return q6off ? below : (x >= L && below);
+    };
     bool lany = false;
     for (int r = (int)lane; r < R; r += G) {
-        uint8_t cr = 0;
-        const uint32_t e1 = m.reac_off[r + 1];
-        for (uint32_t e = m.reac_off[r]; e < e1; e++) {
-            // floor(x / L) < n_c  <=>  x < n_c * L, and floor(x / L) > 0  <=>  x >= L
-            // (x >= 0, L >= 1): the reference's integer test without a division
-            const uint32_t ent = m.reac_ent[e];
-            const uint32_t x = (uint32_t)sl.x((int)(ent >> 8)), L = ent & 0xffu;
-            const bool below = (uint64_t)x < (uint64_t)run.nc * L;
-            if ((fl & F_Q6_OFF) ? below : (x >= L && below)) cr = 1;
+        bool cr = false;
+        const uint2 d = m.reac_desc[r];
+        if (d.x != 0xffffffffu) {
+            cr = (d.x && crit_entry(d.x)) || (d.y && crit_entry(d.y));
+        } else {
+            const uint32_t e1 = m.reac_off[r + 1];
+            for (uint32_t e = m.reac_off[r]; e < e1; e++) cr = crit_entry(m.reac_ent[e]) || cr;
         }
-        sl.cr(r) = cr;
-        lany |= cr != 0;
+        sl.cr(r) = cr ? 1 : 0;
+        lany |= cr;
     }
     const bool anycrit = g.any(lany);
     g.sync();
