@@ -728,12 +728,14 @@ __device__ int decide_step(const Grp<G>& g, const Model& m, const Run& run, cons
         if (e0 == e1) continue;
         float mu = 0.0f, sg = 0.0f;
         for (uint32_t e = e0; e < e1; e++) {
+            // critical reactions add an exact +-0: mu and sg start at +0 and
+            // are never -0, so the sums equal those that skip them
             const uint32_t ent = m.v_ent[e];
             const int r = (int)(ent >> 8);
-            if (sl.cr(r)) continue;
+            const float a = sl.cr(r) ? 0.0f : sl.pa(r);
             const float fv = (float)(int8_t)(ent & 0xffu);
-            mu = mu + fv * sl.pa(r);
-            sg = sg + (fv * fv) * sl.pa(r);
+            mu = mu + fv * a;
+            sg = sg + (fv * fv) * a;
         }
         const int32_t xs = sl.x(s);
         const float gg = gfun(m.hor[s], m.hort[s], xs);
