@@ -460,11 +460,13 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     pl.dec_budget = cfg->dec_budget;
     pl.sched = cfg->sched > 0 ? cfg->sched : 1;
     int G = cfg->group > 0 ? cfg->group : heuristic_group(t);
-    if (cfg->group <= 0) {  // small batches: more lanes per simulation so that every SM gets warps
+    if (cfg->group <= 0) {
+        // small batches (fewer lanes than one 256-thread block per SM): more
+        // lanes per simulation so that every SM gets warps
         DevAttr da0;
         if (device_attr(cfg->device, da0) != CTL_OK) return CTL_ERR_CUDA;
         const int gmax = std::min(t.P, 32);
-        while (G < gmax && (uint64_t)n * G < (uint64_t)2 * 256 * da0.sm_count) G <<= 1;
+        while (G < gmax && (uint64_t)n * G < (uint64_t)256 * da0.sm_count) G <<= 1;
     }
     if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32 && G != 64 && G != 128 && G != 256) {
         set_error("group must be a power of two from 1 to 256");
