@@ -338,6 +338,8 @@ def main():
     ap.add_argument("--sched", type=int, default=0,
                     help="scheduling: 1 block regrouping rounds, 2 warp-local (0 = library choice)")
     ap.add_argument("--flags", type=int, default=0, help="run flags (quirk switches; 1 = forced SSA)")
+    ap.add_argument("--ssa-budget", type=int, default=0, help="SSA steps per simulation and round (0 = library)")
+    ap.add_argument("--dec-budget", type=int, default=0, help="leap decisions per simulation and round (0 = library)")
     ap.add_argument("--autotune", action="store_true", help="measure launch shapes before timing")
     ap.add_argument("--no-autotune", action="store_true", help="config 3: library default shapes")
     ap.add_argument("--no-e2e", action="store_true")
@@ -394,7 +396,8 @@ def main():
         model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
         n = net.n
         cfg = ctl.run_cfg(seed=1 + si, sim_base=rank * n, device=local, group=a.group, threads=a.threads,
-                          min_blocks=a.min_blocks, sched=a.sched, flags=a.flags, uniform_rates=int(bool((net.c == net.c[0]).all())))
+                          min_blocks=a.min_blocks, sched=a.sched, flags=a.flags, ssa_budget=a.ssa_budget,
+                          dec_budget=a.dec_budget, uniform_rates=int(bool((net.c == net.c[0]).all())))
         X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).to(dev)
         c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).to(dev)
         out = torch.empty((n, model.ns, model.s_out), dtype=torch.int32, device=dev)
