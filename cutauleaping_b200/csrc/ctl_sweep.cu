@@ -440,6 +440,9 @@ static bool find_tuned(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, ctl_mod
     return false;
 }
 
+static int default_ssa_budget() { return 16; }
+static int default_dec_budget(int G) { return G > 32 ? 2 : 1; }
+
 static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t n, LaunchPlan& pl,
                               bool sums = false) {
     const HostTables& t = m->t;
@@ -514,6 +517,12 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
         threads -= tstep;
     }
     pl.G = G;
+    // Round budgets when neither the caller nor the tuner chose: 16 SSA steps
+    // and one leap decision per round (one B200, against 8 and 2: +7 % on the
+    // 64 x 128 network, +10 % on Schlogl, +12 % on the uneven batch); groups of
+    // whole warps keep two decisions (512 x 1024: 2.7 % better).
+    if (pl.ssa_budget <= 0) pl.ssa_budget = default_ssa_budget();
+    if (pl.dec_budget <= 0) pl.dec_budget = default_dec_budget(G);
     pl.threads = threads;
     int bps = 0, regs = 0;
     if (ctl_status st = occupancy(dev_id, G, minb, threads, pl.smem, bps, regs); st != CTL_OK) return st;
@@ -547,8 +556,8 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.sim_base = cfg->sim_base;
     run.n = n;
     run.uniform_c = cfg->uniform_rates != 0;
-    run.ssa_budget = pl.ssa_budget > 0 ? (uint32_t)pl.ssa_budget : 8u;
-    run.dec_budget = pl.dec_budget > 0 ? (uint32_t)pl.dec_budget : 2u;
+    run.ssa_budget = (uint32_t)pl.ssa_budget;
+    run.dec_budget = (uint32_t)pl.dec_budget;
     run.warp_local = pl.sched == 2 ? 1u : 0u;
     run.X0 = dX0;
     run.c = dc;
@@ -643,8 +652,8 @@ extern "C" ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uin
     li->sm_count = pl.sm_count;
     li->min_blocks = pl.minb;
     li->sched = pl.sched;
-    li->ssa_budget = pl.ssa_budget > 0 ? pl.ssa_budget : 8;
-    li->dec_budget = pl.dec_budget > 0 ? pl.dec_budget : 2;
+    li->ssa_budget = pl.ssa_budget;
+    li->dec_budget = pl.dec_budget;
     return CTL_OK;
 }
 
@@ -827,35 +836,42 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         cudaEventElapsedTime(&ms, e0, e1);
         return CTL_OK;
     };
-    int bestG = heuristic_group(t), bestT = 256, bestS = 8, bestD = 2, bestM = 2, bestC = 1;
+    const int S0 = default_ssa_budget();
+    int bestG = heuristic_group(t), bestT = 256, bestS = S0, bestD = default_dec_budget(bestG), bestM = 2, bestC = 1;
     float best_ms = 3.4e38f;
     if (e == cudaSuccess) {
         for (int G = 1; G <= 256 && G <= t.P; G <<= 1) {  // 1. lanes per simulation
             float ms;
-            if (time_shape(G, 256, 8, 2, 2, 1, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestG = G; }
+            if (time_shape(G, 256, S0, default_dec_budget(G), 2, 1, ms) == CTL_OK && ms < best_ms) {
+                best_ms = ms;
+                bestG = G;
+                bestD = default_dec_budget(G);
+            }
         }
         for (int th : {64, 128, 192}) {                   // 2. threads per block
             float ms;
-            if (th % bestG == 0 && th >= bestG && time_shape(bestG, th, 8, 2, 2, 1, ms) == CTL_OK && ms < best_ms) {
+            if (th % bestG == 0 && th >= bestG && time_shape(bestG, th, S0, bestD, 2, 1, ms) == CTL_OK &&
+                ms < best_ms) {
                 best_ms = ms;
                 bestT = th;
             }
         }
         {                                                  // 3. scheduling: warp-local vs block rounds
             float ms;
-            if (time_shape(bestG, bestT, 8, 2, 2, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestC = 2; }
+            if (time_shape(bestG, bestT, S0, bestD, 2, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestC = 2; }
         }
         for (int mb : {3, 4}) {                            // 4. register budget (resident blocks)
             float ms;
-            if (time_shape(bestG, bestT, 8, 2, mb, bestC, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestM = mb; }
+            if (time_shape(bestG, bestT, S0, bestD, mb, bestC, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestM = mb; }
         }
-        for (int sb : {2, 4, 16, 32}) {                    // 5. SSA steps per round
+        for (int sb : {4, 8, 32}) {                        // 5. SSA steps per round
             float ms;
-            if (time_shape(bestG, bestT, sb, 2, bestM, bestC, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestS = sb; }
+            if (time_shape(bestG, bestT, sb, bestD, bestM, bestC, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestS = sb; }
         }
-        for (int db : {1, 4, 8}) {                         // 6. decisions per round
+        const int D0 = bestD;
+        for (int db : {1, 2, 4}) {                         // 6. decisions per round
             float ms;
-            if (time_shape(bestG, bestT, bestS, db, bestM, bestC, ms) == CTL_OK && ms < best_ms) {
+            if (db != D0 && time_shape(bestG, bestT, bestS, db, bestM, bestC, ms) == CTL_OK && ms < best_ms) {
                 best_ms = ms;
                 bestD = db;
             }
