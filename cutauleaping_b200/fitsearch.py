@@ -262,7 +262,7 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
     `finetune_reps` of the trajectories just simulated for half of those
     candidates (fresh optimiser moments, constant rate, half of every batch
     replayed from `replay` = the original training data when given), and the
-    simulated fitness of the other half judges the result: the fine-tuned
+    simulated fitness of the other half decides the outcome: the fine-tuned
     weights are kept only if the surrogate's error on that half went down.
     Every candidate whose fitness is reported was simulated.  Returns a list
     of (wall seconds, simulations so far, best true fitness, best theta), one

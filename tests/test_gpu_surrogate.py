@@ -72,7 +72,7 @@ def test_search_runs_and_records_budget(trained, inner):
 
 
 def test_guarded_finetuning_keeps_or_restores(trained):
-    """Fine-tuning on re-simulated trajectories is judged by simulated
+    """Fine-tuning on re-simulated trajectories is checked against simulated
     fitness on held-out candidates: the log says whether the new weights were
     kept, and a rejected phase leaves the surrogate's predictions unchanged."""
     import torch
