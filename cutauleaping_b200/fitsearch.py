@@ -29,6 +29,7 @@ import numpy as np
 
 from . import CtlError, Model, OK, lib, run_cfg
 from . import inputs
+from . import shard
 from . import surrogate as sg
 
 
@@ -146,15 +147,22 @@ def training_data(p: FitProblem, n_traj, *, seed=5, sim_seed=91):
 
 
 def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-3, seed=0, log=None,
-                    net=None, sc=None, steps=None, cosine=True, replay=None):
+                    net=None, sc=None, steps=None, cosine=True, replay=None, dist=None):
     """Fit the MLP to (theta, t) -> counts of single trajectories (Gaussian
     NLL: the network learns the ensemble mean and log-variance).  With `net`
     and `sc` given, continues training that network (fine-tuning) with its
     output scaling unchanged; with `replay` = (theta0, traj0), half of every
     batch is drawn from that earlier data so the network keeps what it knew
-    outside the new data's region."""
+    outside the new data's region.
+
+    Data-parallel with `dist` (an initialised process group of several
+    ranks, each holding its own shard of the trajectories): every rank
+    draws its own batch, the gradients are averaged over ranks in one
+    all-reduce before each Adam step (shard.allreduce_mean), and the output
+    scaling is rank 0's, so all ranks keep identical weights."""
     import torch
     n, ns, S = traj.shape
+    rank = dist.get_rank() if shard.multi_rank(dist) else 0
     if sc is None:
         # per-species scale from a sample of the trajectories
         ix = torch.randint(0, n, (min(n, 1 << 14),), device="cuda",
@@ -162,6 +170,7 @@ def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-
         ys = traj[ix].to(torch.float32)
         y_mean = ys.mean(dim=(0, 1))
         y_std = ys.std(dim=(0, 1)).clamp_min(1.0)
+        shard.broadcast_([y_mean, y_std], dist)
         sc = sg.Scaling(p.log_lo, p.log_hi, float(p.tvec[-1]), y_mean.cpu().numpy(), y_std.cpu().numpy())
     else:
         y_mean = torch.as_tensor(sc.y_mean, dtype=torch.float32, device="cuda")
@@ -171,7 +180,7 @@ def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-
         net = sg.MLP(S, seed=seed)
     total = n * ns
     steps = steps or max(1, (epochs * total) // batch)
-    g = torch.Generator(device="cuda").manual_seed(seed + net.version)
+    g = torch.Generator(device="cuda").manual_seed(seed + net.version + 7919 * rank)
     sources = [(theta, traj, batch if replay is None else batch // 2)]
     if replay is not None:
         sources.append((replay[0], replay[1], batch - batch // 2))
@@ -187,6 +196,7 @@ def train_surrogate(p: FitProblem, theta, traj, *, epochs=1, batch=16384, lr=2e-
         tgt = Ts[0] if len(Ts) == 1 else torch.cat(Ts)
         out = net.forward(X)
         loss, dW, db = net.backward(out, tgt)
+        shard.allreduce_mean(dW + db, dist)
         rate = lr * 0.5 * (1 + math.cos(math.pi * it / steps)) if cosine else lr
         net.adam(dW, db, lr=rate)
         if log is not None and (it % 200 == 0 or it == steps - 1):

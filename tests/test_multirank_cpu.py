@@ -65,3 +65,76 @@ def test_two_ranks_reproduce_single_process(tmp_path):
         assert np.allclose(r["mean"], mean, rtol=0, atol=1e-9)
         assert np.allclose(r["var"], var, rtol=1e-12, atol=1e-9)
         assert float(r["slow"]) == 20.0
+
+
+def _dp_worker(rank, world, port, out_dir):
+    """Data-parallel training step on CPU: each rank takes its shard of one
+    batch, the gradients are averaged with shard.allreduce_mean, and every
+    rank applies the same update."""
+    import torch
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # the averaging itself, on tensors of several shapes
+        a = torch.full((3, 4), float(rank + 1))
+        b = torch.arange(5, dtype=torch.float32) * (rank + 1)
+        shard.allreduce_mean([a, b], dist)
+        # rank 0's scaling wins
+        sc = torch.tensor([float(rank) + 0.5, 2.0 * rank])
+        shard.broadcast_([sc], dist)
+        # a linear least-squares model trained by gradient descent
+        g = torch.Generator().manual_seed(4)
+        X = torch.randn(64, 5, generator=g, dtype=torch.float64)
+        y = X @ torch.tensor([1.0, -2.0, 0.5, 3.0, -1.0], dtype=torch.float64) + 0.1
+        off, cnt = shard.shard_range(64, rank, world)
+        w = torch.zeros(5, dtype=torch.float64, requires_grad=True)
+        c = torch.zeros(1, dtype=torch.float64, requires_grad=True)
+        for _ in range(20):
+            loss = ((X[off:off + cnt] @ w + c - y[off:off + cnt]) ** 2).mean()
+            gw, gc = torch.autograd.grad(loss, [w, c])
+            gw, gc = gw.clone(), gc.clone()
+            shard.allreduce_mean([gw, gc], dist)
+            with torch.no_grad():
+                w -= 0.1 * gw
+                c -= 0.1 * gc
+        np.savez(os.path.join(out_dir, f"dp{rank}.npz"), a=a.numpy(), b=b.numpy(), sc=sc.numpy(),
+                 w=w.detach().numpy(), c=c.detach().numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_data_parallel_gradient_average(tmp_path):
+    """Two ranks, each with half of the batch, take the same steps as one
+    process with the whole batch (equal shards: the mean of the shard means
+    is the batch mean)."""
+    import torch
+    port = _free_port()
+    mp.start_processes(_dp_worker, args=(2, port, str(tmp_path)), nprocs=2, start_method="spawn", join=True)
+    r0, r1 = (np.load(tmp_path / f"dp{r}.npz") for r in range(2))
+    for r in (r0, r1):
+        assert np.array_equal(r["a"], np.full((3, 4), 1.5, np.float32))
+        assert np.array_equal(r["b"], np.arange(5, dtype=np.float32) * 1.5)
+        assert np.array_equal(r["sc"], np.array([0.5, 0.0], np.float32))
+    assert np.array_equal(r0["w"], r1["w"]) and np.array_equal(r0["c"], r1["c"])
+    g = torch.Generator().manual_seed(4)
+    X = torch.randn(64, 5, generator=g, dtype=torch.float64)
+    y = X @ torch.tensor([1.0, -2.0, 0.5, 3.0, -1.0], dtype=torch.float64) + 0.1
+    w = torch.zeros(5, dtype=torch.float64, requires_grad=True)
+    c = torch.zeros(1, dtype=torch.float64, requires_grad=True)
+    for _ in range(20):
+        loss = ((X @ w + c - y) ** 2).mean()
+        gw, gc = torch.autograd.grad(loss, [w, c])
+        with torch.no_grad():
+            w -= 0.1 * gw
+            c -= 0.1 * gc
+    assert np.allclose(r0["w"], w.detach().numpy(), rtol=1e-12, atol=1e-12)
+    assert np.allclose(r0["c"], c.detach().numpy(), rtol=1e-12, atol=1e-12)
+
+
+def test_single_rank_helpers_are_no_ops():
+    import torch
+    t = torch.arange(4, dtype=torch.float32)
+    assert shard.allreduce_mean([t], None)[0] is t and np.array_equal(t.numpy(), np.arange(4))
+    assert not shard.multi_rank(None)
+    assert shard.broadcast_([t], None)[0] is t
