@@ -40,7 +40,7 @@ EXPORTS = [
     "ctl_status_str", "ctl_last_error", "ctl_model_load", "ctl_model_create", "ctl_model_free",
     "ctl_model_dims_get", "ctl_model_hor", "ctl_rows_load", "ctl_run_cfg_default", "ctl_run",
     "ctl_run_device", "ctl_run_device_noalloc", "ctl_launch_query", "ctl_autotune", "ctl_graph_create", "ctl_graph_launch", "ctl_graph_free",
-    "ctl_write_dynamics", "ctl_print_dynamics", "ctl_target_load", "ctl_target_free",
+    "ctl_write_dynamics", "ctl_print_dynamics", "ctl_write_samples_binary", "ctl_target_load", "ctl_target_free",
     "ctl_target_dims", "ctl_fitness", "ctl_fitness_device", "ctl_mlp_gemm", "ctl_mlp_nll_grad", "ctl_mlp_colsum",
     "ctl_mlp_adam", "ctl_mlp_pack_bytes", "ctl_mlp_pack", "ctl_mlp_screen", "ctl_run_device_sums",
     "ctl_fitness_sums_device", "ctl_fitness_run",
@@ -115,6 +115,7 @@ def lib():
         L.ctl_graph_free.restype = None
         L.ctl_write_dynamics.argtypes = [P, C.c_char_p, C.c_uint32, P, C.c_uint32, C.c_int32]
         L.ctl_print_dynamics.argtypes = [P, C.c_uint32, P]
+        L.ctl_write_samples_binary.argtypes = [P, C.c_char_p, C.c_uint32, P, C.c_uint32]
         L.ctl_target_load.argtypes = [C.c_char_p, P, C.c_uint32, C.c_uint32, C.POINTER(P)]
         L.ctl_target_free.argtypes = [P]
         L.ctl_target_free.restype = None
@@ -246,6 +247,13 @@ class Model:
         _check(lib().ctl_write_dynamics(self._h, os.fsencode(path_prefix), samples.shape[0],
                                         _p(samples), first_id, threads), "ctl_write_dynamics")
 
+    def write_samples_binary(self, path: str, samples, first_id=0):
+        """The whole batch in one binary file (ctl_write_samples_binary);
+        read it back with read_samples_binary."""
+        samples = np.ascontiguousarray(samples, dtype=np.uint32)
+        _check(lib().ctl_write_samples_binary(self._h, os.fsencode(path), samples.shape[0], _p(samples),
+                                              first_id), "ctl_write_samples_binary")
+
 
 class Graph:
     """A captured sweep (ctl_graph); replay with launch()."""
@@ -261,6 +269,35 @@ class Graph:
         if h is not None and h.value and _lib is not None:
             _lib.ctl_graph_free(h)
             self._h = None
+
+
+SAMPLES_MAGIC = b"CTLSAMP1"
+
+
+def read_samples_binary(path: str, mmap: bool = True):
+    """Read a file written by ctl_write_samples_binary (or the CLI with
+    CTL_BINARY_OUTPUT=1): returns dict(t [ns] float64, species [s_out],
+    first_id, samples [n][ns][s_out] uint32 -- memory-mapped unless mmap is
+    False).  Raises ValueError on a file of another format or a short file."""
+    with open(path, "rb") as f:
+        head = f.read(24)
+        if len(head) < 24 or head[:8] != SAMPLES_MAGIC:
+            raise ValueError(f"{path}: not a sample file (magic {head[:8]!r})")
+        n, ns, s_out, first_id = np.frombuffer(head, dtype="<u4", offset=8, count=4).tolist()
+        t = np.frombuffer(f.read(8 * ns), dtype="<f8")
+        species = np.frombuffer(f.read(4 * s_out), dtype="<u4")
+        if t.size != ns or species.size != s_out:
+            raise ValueError(f"{path}: truncated header")
+    data_off = (24 + 8 * ns + 4 * s_out + 15) // 16 * 16
+    need = data_off + 4 * n * ns * s_out
+    if os.path.getsize(path) != need:
+        raise ValueError(f"{path}: {os.path.getsize(path)} bytes, the header announces {need}")
+    shape = (n, ns, s_out)
+    if mmap and n * ns * s_out:
+        samples = np.memmap(path, dtype="<u4", mode="r", offset=data_off, shape=shape)
+    else:
+        samples = np.fromfile(path, dtype="<u4", count=n * ns * s_out, offset=data_off).reshape(shape)
+    return {"t": t.copy(), "species": species.copy(), "first_id": first_id, "samples": samples}
 
 
 def load_rows(folder: str, model: Model, offset: int, n: int):

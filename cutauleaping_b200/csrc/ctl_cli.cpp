@@ -17,6 +17,9 @@
 //   CTL_OUTPUT_EXISTING_OK=1  write into an existing output folder instead of
 //                  falling back to "./" (the reference falls back on any
 //                  mkdir failure, tau.cu:3133-3139)
+//   CTL_BINARY_OUTPUT=1  one binary file <output_folder><prefix>.ctlbin
+//                  (ctl_write_samples_binary) instead of a text file per
+//                  simulation
 #include <sys/stat.h>
 #include <sys/types.h>
 
@@ -185,7 +188,12 @@ int main(int argc, const char* argv[]) {
 
     std::string dumpfile = out_dir + prefix;
     if (!just_fitness) {
-        if (!stdout_dyn) {
+        if (!stdout_dyn && env_u("CTL_BINARY_OUTPUT", 0) == 1) {
+            const std::string bin = dumpfile + ".ctlbin";
+            printf(" * Writing dynamics to file %s\n", bin.c_str());
+            fflush(stdout);
+            st = ctl_write_samples_binary(model, bin.c_str(), N, samples.data(), 0);
+        } else if (!stdout_dyn) {
             printf(" * Writing dynamics to file %s\n", dumpfile.c_str());
             fflush(stdout);
             st = ctl_write_dynamics(model, dumpfile.c_str(), N, samples.data(), 0, 0);

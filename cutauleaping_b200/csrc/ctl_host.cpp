@@ -428,6 +428,38 @@ extern "C" ctl_status ctl_print_dynamics(const ctl_model* m, uint32_t n, const u
     return CTL_OK;
 }
 
+extern "C" ctl_status ctl_write_samples_binary(const ctl_model* m, const char* path, uint32_t n,
+                                               const uint32_t* samples, uint32_t first_id) {
+    if (!m || !path || (!samples && n)) return fail(CTL_ERR_ARG, "null argument");
+    const HostTables& t = m->t;
+    std::vector<unsigned char> head;
+    auto put = [&head](const void* p, size_t k) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        head.insert(head.end(), b, b + k);
+    };
+    put("CTLSAMP1", 8);
+    const uint32_t dims[4] = {n, (uint32_t)t.ns, (uint32_t)t.s_out, first_id};
+    put(dims, sizeof(dims));
+    put(t.tvec.data(), t.tvec.size() * sizeof(double));
+    for (int k = 0; k < t.s_out; k++) {
+        const uint32_t sp = (size_t)k < t.cs.size() ? t.cs[k] : (uint32_t)k;
+        put(&sp, sizeof(sp));
+    }
+    head.resize((head.size() + 15) & ~(size_t)15, 0);
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return fail(CTL_ERR_IO, std::string("cannot write ") + path);
+    bool ok = std::fwrite(head.data(), 1, head.size(), fp) == head.size();
+    const size_t bytes = (size_t)n * t.ns * t.s_out * sizeof(uint32_t);
+    const size_t piece = (size_t)64 << 20;
+    for (size_t off = 0; ok && off < bytes; off += piece) {
+        const size_t k = std::min(piece, bytes - off);
+        ok = std::fwrite(reinterpret_cast<const unsigned char*>(samples) + off, 1, k, fp) == k;
+    }
+    ok = (std::fclose(fp) == 0) && ok;
+    if (!ok) return fail(CTL_ERR_IO, std::string("cannot write ") + path);
+    return CTL_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Fitness targets (read_time_series, tau.cu:1056-1261)
 // ---------------------------------------------------------------------------

@@ -197,6 +197,14 @@ ctl_status ctl_write_dynamics(const ctl_model* m, const char* path_prefix, uint3
 /* PrintDynamics2 (tau.cu:3472-3507): the same rows to stdout, a blank line
  * after each simulation. */
 ctl_status ctl_print_dynamics(const ctl_model* m, uint32_t n, const uint32_t* samples);
+/* One binary file for the whole batch instead of WriteDynamics2's text file
+ * per simulation (tau.cu:3431-3469), for batches where text output would
+ * dominate the run.  Little-endian layout: the 8 bytes "CTLSAMP1"; uint32 n,
+ * ns, s_out, first_id; float64 t[ns]; uint32 species[s_out] (the sampled
+ * species' indices); zero bytes up to a multiple of 16; then uint32
+ * samples[n][ns][s_out] exactly as ctl_run returns them. */
+ctl_status ctl_write_samples_binary(const ctl_model* m, const char* path, uint32_t n,
+                                    const uint32_t* samples, uint32_t first_id);
 
 /* ---- fitness ------------------------------------------------------------- */
 /* read_time_series (tau.cu:1056-1261): ts_rep, p_rep, ts_numtgt, tts_vector,

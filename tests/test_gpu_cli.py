@@ -4,7 +4,8 @@
 verbose` (kernel.cu:74-436) must write the per-simulation files of
 WriteDynamics2 (2phase_n-tau-leaping.cu:3431-3469) with the oracle's samples,
 honour `offset` (rows and random streams of a larger run), force SSA, print
-dynamics to stdout with verbose = 2, and print calculateFitness
+dynamics to stdout with verbose = 2, write one binary sample file with
+CTL_BINARY_OUTPUT=1, and print calculateFitness
 (3324-3408) values in fitness mode 2 -- checked against a numpy restatement.
 """
 import os
@@ -45,6 +46,19 @@ def test_cli_files_match_oracle(folder, tmp_path, force):
     for gid in range(32):
         got = open(tmp_path / "out" / f"pref_{gid}").read()
         assert got == _rows(net.tvec, ref[gid]), f"simulation {gid}"
+
+
+def test_cli_binary_output_matches_oracle(folder, tmp_path):
+    """CTL_BINARY_OUTPUT=1: one <prefix>.ctlbin with the same samples the
+    text files carry, and no per-simulation files."""
+    path, net = folder
+    p = _cli([path, 8, 2, 0, 8, tmp_path / "ob", "pref", 0, 0, 0], {"CTL_BINARY_OUTPUT": "1"})
+    assert p.returncode == 0, p.stderr
+    ref, _ = oracle_model(net, seed=5).run(net.X0[8:24], net.c[8:24].astype(np.float32), sim_base=8)
+    d = ctl.read_samples_binary(str(tmp_path / "ob" / "pref.ctlbin"))
+    assert np.array_equal(np.asarray(d["samples"]), ref)
+    assert np.array_equal(d["t"], np.asarray(net.tvec, np.float64))
+    assert sorted(os.listdir(tmp_path / "ob")) == ["pref.ctlbin"]
 
 
 def test_cli_stdout_dynamics(folder, tmp_path):

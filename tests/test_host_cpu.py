@@ -171,3 +171,35 @@ def test_run_cfg_rejected_before_any_device_work(kw):
     with pytest.raises(ctl.CtlError) as e:
         m.run(net.X0, net.c, **kw)
     assert e.value.status == ctl.ERR_ARG
+
+
+@pytest.mark.parametrize("with_cs", [True, False])
+def test_binary_samples_roundtrip(tmp_path, with_cs):
+    """ctl_write_samples_binary: header (instants, sampled species, first id),
+    16-byte aligned payload identical to the samples given, and the reader's
+    checks on foreign or truncated files."""
+    net = inputs.schlogl(5, samples=9, t_end=1.0)
+    cs = net.cs if with_cs else None
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, cs)
+    so = m.s_out
+    rng = np.random.default_rng(1)
+    samples = rng.integers(0, 2**32 - 1, size=(5, 9, so), dtype=np.uint64).astype(np.uint32)
+    path = str(tmp_path / "batch.ctlbin")
+    m.write_samples_binary(path, samples, first_id=40)
+    d = ctl.read_samples_binary(path)
+    assert d["first_id"] == 40
+    assert np.array_equal(d["t"], np.asarray(net.tvec, np.float64))
+    assert np.array_equal(d["species"], np.asarray(cs if with_cs else np.arange(so), np.uint32))
+    assert np.array_equal(np.asarray(d["samples"]), samples)
+    raw = open(path, "rb").read()
+    off = (24 + 8 * 9 + 4 * so + 15) // 16 * 16
+    assert len(raw) == off + samples.nbytes and raw[off:] == samples.tobytes()
+    assert ctl.read_samples_binary(path, mmap=False)["samples"].tolist() == samples.tolist()
+    open(tmp_path / "short", "wb").write(raw[:-4])
+    with pytest.raises(ValueError):
+        ctl.read_samples_binary(str(tmp_path / "short"))
+    open(tmp_path / "text", "wb").write(b"0.1\t5\n" * 10)
+    with pytest.raises(ValueError):
+        ctl.read_samples_binary(str(tmp_path / "text"))
+    with pytest.raises(ctl.CtlError):
+        m.write_samples_binary(str(tmp_path / "no_such_dir" / "x"), samples)
