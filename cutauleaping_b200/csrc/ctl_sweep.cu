@@ -444,10 +444,10 @@ static int default_ssa_budget() { return 16; }
 static int default_dec_budget(int G) { return G > 32 ? 2 : 1; }
 
 static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t n, LaunchPlan& pl,
-                              bool sums = false) {
+                              bool sums = false, bool use_tuned = true) {
     const HostTables& t = m->t;
     ctl_run_cfg tuned_cfg = *cfg_in;
-    if (cfg_in->group <= 0 && cfg_in->threads <= 0) {
+    if (use_tuned && cfg_in->group <= 0 && cfg_in->threads <= 0) {
         ctl_model::Tuned e;
         if (find_tuned(m, cfg_in, n, e)) {
             tuned_cfg.group = e.group;
@@ -794,11 +794,12 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
     return CTL_OK;
 }
 
-// Measured autotuner: times candidate launch shapes on the first `sample`
-// simulations of the batch (results are identical for every shape, only the
-// time differs) -- group size first, then threads per block, then the
-// per-round budgets -- and caches the fastest for this (device, batch-size
-// bucket, rate mode, flags).
+// Measured autotuner: times the library's own plan, then candidate launch
+// shapes greedily on the first `sample` simulations of the batch (results
+// are identical for every shape, only the time differs) -- group size,
+// threads per block, scheduling, register budget, then the per-round
+// budgets -- and caches the fastest for this (device, batch-size bucket,
+// rate mode, flags).  Nothing slower than the library's plan is cached.
 extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* d_X0,
                                    const float* d_c, uint32_t sample, ctl_launch_info* best) {
     if (!m || !d_X0 || !d_c || n == 0) return CTL_ERR_ARG;
@@ -808,7 +809,23 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
     DeviceGuard dg(cfg->device);
     DeviceCopy* d = nullptr;
     if ((st = ensure_device(m, cfg->device, d)) != CTL_OK) return st;
-    const uint32_t k = sample == 0 || sample > n ? n : sample;
+    // The library's own plan for this batch (heuristic shape, default
+    // budgets, no earlier tuning) is the incumbent every candidate must beat.
+    ctl_run_cfg c0 = *cfg;
+    c0.group = 0;
+    c0.threads = 0;
+    c0.min_blocks = 0;
+    c0.sched = 0;
+    c0.ssa_budget = 0;
+    c0.dec_budget = 0;
+    LaunchPlan p0;
+    if ((st = plan_launch(m, &c0, n, p0, false, false)) != CTL_OK) return st;
+    // A sample of about one wave of resident simulations is timed mostly by
+    // its slowest simulations and favours shapes with short tails; at least
+    // four waves (or the whole batch) weigh the steady state as the full
+    // batch does.
+    uint32_t k = sample == 0 || sample > n ? n : sample;
+    k = (uint32_t)std::min<uint64_t>(n, std::max<uint64_t>(k, 4ull * (uint64_t)p0.blocks * (uint64_t)p0.NS));
     cudaStream_t s;
     CTL_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     void *dout = nullptr, *dinf = nullptr;
@@ -826,7 +843,7 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         c.min_blocks = mb;
         c.sched = sc;
         LaunchPlan pl;
-        ctl_status r = plan_launch(m, &c, k, pl);
+        ctl_status r = plan_launch(m, &c, k, pl, false, false);
         if (r != CTL_OK) return r;
         cudaEventRecord(e0, s);
         r = enqueue_sweep(m, &c, k, d_X0, d_c, static_cast<uint32_t*>(dout), static_cast<ctl_sim_info*>(dinf), s, pl, *d);
@@ -837,36 +854,53 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         return CTL_OK;
     };
     const int S0 = default_ssa_budget();
-    int bestG = heuristic_group(t), bestT = 256, bestS = S0, bestD = default_dec_budget(bestG), bestM = 2, bestC = 1;
+    int bestG = p0.G, bestT = p0.threads, bestS = p0.ssa_budget, bestD = p0.dec_budget, bestM = p0.minb,
+        bestC = p0.sched;
     float best_ms = 3.4e38f;
     if (e == cudaSuccess) {
+        {                                                  // 0. the library's own plan
+            float ms;
+            if (time_shape(bestG, bestT, bestS, bestD, bestM, bestC, ms) == CTL_OK) best_ms = ms;
+        }
         for (int G = 1; G <= 256 && G <= t.P; G <<= 1) {  // 1. lanes per simulation
             float ms;
-            if (time_shape(G, 256, S0, default_dec_budget(G), 2, 1, ms) == CTL_OK && ms < best_ms) {
+            if (G != p0.G && time_shape(G, 256, S0, default_dec_budget(G), 2, 1, ms) == CTL_OK && ms < best_ms) {
                 best_ms = ms;
                 bestG = G;
+                bestT = 256;
+                bestS = S0;
                 bestD = default_dec_budget(G);
+                bestM = 2;
+                bestC = 1;
             }
         }
-        for (int th : {64, 128, 192}) {                   // 2. threads per block
+        for (int th : {64, 128, 192, 256}) {              // 2. threads per block
             float ms;
-            if (th % bestG == 0 && th >= bestG && time_shape(bestG, th, S0, bestD, 2, 1, ms) == CTL_OK &&
-                ms < best_ms) {
+            if (th != bestT && th % bestG == 0 && th >= bestG &&
+                time_shape(bestG, th, bestS, bestD, bestM, bestC, ms) == CTL_OK && ms < best_ms) {
                 best_ms = ms;
                 bestT = th;
             }
         }
         {                                                  // 3. scheduling: warp-local vs block rounds
             float ms;
-            if (time_shape(bestG, bestT, S0, bestD, 2, 2, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestC = 2; }
+            const int sc = bestC == 2 ? 1 : 2;
+            if (time_shape(bestG, bestT, bestS, bestD, bestM, sc, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestC = sc; }
         }
-        for (int mb : {3, 4}) {                            // 4. register budget (resident blocks)
+        for (int mb : {2, 3, 4}) {                         // 4. register budget (resident blocks)
             float ms;
-            if (time_shape(bestG, bestT, S0, bestD, mb, bestC, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestM = mb; }
+            if (mb != bestM && time_shape(bestG, bestT, bestS, bestD, mb, bestC, ms) == CTL_OK && ms < best_ms) {
+                best_ms = ms;
+                bestM = mb;
+            }
         }
-        for (int sb : {4, 8, 32}) {                        // 5. SSA steps per round
+        const int S1 = bestS;
+        for (int sb : {4, 8, 16, 32}) {                    // 5. SSA steps per round
             float ms;
-            if (time_shape(bestG, bestT, sb, bestD, bestM, bestC, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestS = sb; }
+            if (sb != S1 && time_shape(bestG, bestT, sb, bestD, bestM, bestC, ms) == CTL_OK && ms < best_ms) {
+                best_ms = ms;
+                bestS = sb;
+            }
         }
         const int D0 = bestD;
         for (int db : {1, 2, 4}) {                         // 6. decisions per round

@@ -174,9 +174,11 @@ ctl_status ctl_run_device_noalloc(ctl_model* m, const ctl_run_cfg* cfg, uint32_t
                                   const int32_t* d_X0, const float* d_c, uint32_t* d_samples,
                                   ctl_sim_info* d_info, void* stream);
 
-/* Measured autotuner: times candidate shapes (lanes per simulation, threads
- * per block, per-round budgets) on the first `sample` simulations of the
- * batch on device buffers and caches the fastest; later calls with
+/* Measured autotuner: times the library's own plan and candidate shapes
+ * (lanes per simulation, threads per block, scheduling, register budget,
+ * per-round budgets) on the first `sample` simulations of the batch on
+ * device buffers -- at least four waves of resident simulations, or the
+ * whole batch -- and caches the fastest; later calls with
  * group == threads == 0 use it.  Never changes results. */
 ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* d_X0,
                         const float* d_c, uint32_t sample, ctl_launch_info* best);

@@ -145,3 +145,26 @@ def test_host_run_with_overlapped_copies_matches_device_run():
     sub = net.subset(slice(2300, 2304))
     out_o, info_o = oracle_run(sub, seed=3, sim_base=2300)
     assert np.array_equal(out_h[2300:2304], out_o)
+
+
+def test_autotune_caches_a_shape_and_keeps_results():
+    """ctl_autotune times the library's plan and its candidates, caches the
+    winner for this batch size, and later calls with group == threads == 0
+    run that shape with the same results as the untuned plan."""
+    import torch
+    from cutauleaping_b200 import inputs
+    net = inputs.schlogl(3000, samples=20, t_end=2.0)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    cfg = ctl.run_cfg(seed=17)
+    before = m.launch_info(net.n, cfg)
+    ref, ref_info = m.run(net.X0, net.c, cfg)
+    X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).cuda()
+    c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).cuda()
+    best = m.autotune(net.n, X0.data_ptr(), c.data_ptr(), sample=64, cfg=cfg)
+    after = m.launch_info(net.n, cfg)
+    for f in ("group", "threads", "min_blocks", "sched", "ssa_budget", "dec_budget"):
+        assert getattr(after, f) == getattr(best, f), f
+    assert best.group in (1, 2, 4) and best.min_blocks in (2, 3, 4) and best.sched in (1, 2)
+    out, info = m.run(net.X0, net.c, cfg)
+    assert np.array_equal(out, ref) and same_info(info, ref_info) is None
+    assert before.group >= 1
