@@ -75,7 +75,6 @@ def test_guarded_finetuning_keeps_or_restores(trained):
     """Fine-tuning on re-simulated trajectories is checked against simulated
     fitness on held-out candidates: the log says whether the new weights were
     kept, and a rejected phase leaves the surrogate's predictions unchanged."""
-    import torch
     from cutauleaping_b200 import fitsearch as fs
     p, net, sc, _ = trained
     theta, traj = fs.training_data(p, 1 << 12, seed=9)

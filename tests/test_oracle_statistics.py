@@ -67,6 +67,11 @@ def test_pure_decay_ssa_is_binomial():
         x = out[:, i].astype(float)
         assert abs(x.mean() - N0 * p) < 4 * math.sqrt(N0 * p * (1 - p) / n)
         assert abs(x.var() / (N0 * p * (1 - p)) - 1) < 4 * math.sqrt(2 / n)
+        # whole distribution: Kolmogorov distance to Binomial(N0, p) within
+        # the 1 % critical value (conservative for a discrete law)
+        k = np.arange(N0 + 1)
+        emp = np.searchsorted(np.sort(x), k, side="right") / n
+        assert np.max(np.abs(emp - binom.cdf(k, N0, p))) < 1.63 / math.sqrt(n)
 
 
 def test_immigration_death_tau_leaping_mean():
