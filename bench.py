@@ -15,6 +15,9 @@ CUDA graph (work-queue reset + persistent kernel).
   e2e       the same metric through the C ABI call a user makes (ctl_run) with
             pinned host buffers: H2D of X0/c, the sweep, D2H of all samples and
             per-simulation records, timed on the host around the call.
+  io        output files timed apart from the sweep (rank 0, up to 4,096
+            simulations' samples): the reference's text file per simulation
+            against the one-file binary dump, seconds and bytes per simulation.
   --impl reference
             the reference routine on the host cores: the C restatement in
             oracle/ (the reference has no CPU implementation of its own), all
@@ -90,6 +93,35 @@ def algorithmic_bytes(net):
     (4 ns s_out) + its 40-byte record."""
     so = net.S if net.cs is None else len(net.cs)
     return 4 * net.S + 4 * net.R + 4 * len(net.tvec) * so + 40
+
+
+def io_timing(model, samples, threads: int = 0):
+    """Output-file cost, timed apart from the sweep: the reference's text file
+    per simulation (ctl_write_dynamics, WriteDynamics2's format) and the
+    one-file binary dump (ctl_write_samples_binary) for `samples`
+    [n][ns][s_out], written to a temporary folder that is removed after.
+    Returns seconds per simulation for each, or the error when the host
+    cannot write."""
+    import shutil
+    import tempfile
+    n = int(samples.shape[0])
+    d = tempfile.mkdtemp(prefix="ctl_io_")
+    try:
+        t0 = time.perf_counter()
+        model.write_dynamics(os.path.join(d, "pref"), samples, threads=threads)
+        t1 = time.perf_counter()
+        model.write_samples_binary(os.path.join(d, "batch.ctlbin"), samples)
+        t2 = time.perf_counter()
+        text_bytes = sum(e.stat().st_size for e in os.scandir(d) if e.name.startswith("pref_"))
+        return {"sample_sims": n, "threads": threads or os.cpu_count(),
+                "text_s_per_sim": (t1 - t0) / n, "binary_s_per_sim": (t2 - t1) / n,
+                "text_bytes_per_sim": text_bytes / n,
+                "binary_bytes_per_sim": os.path.getsize(os.path.join(d, "batch.ctlbin")) / n,
+                "folder": "temporary folder on the host's default temp file system"}
+    except Exception as e:  # a full or read-only disk must not end the benchmark
+        return {"error": f"{type(e).__name__}: {e}"}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
 
 
 class ClockSampler:
@@ -344,6 +376,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="config 3: library default shapes")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-io", action="store_true", help="skip timing the output files")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -525,6 +558,14 @@ def main():
         cpu = {"value": v, "unit": "sims/s", "cores": meta["cores"], "kind": "port",
                "sample": meta["sample"], "firings_per_s": fv}
 
+    io = None
+    if rank == 0 and not a.no_io:
+        pt = parts[0]
+        k = min(pt["net"].n, 4096)
+        io = io_timing(pt["model"], pt["out"][:k].cpu().numpy().view(np.uint32))
+        if "error" not in io:
+            io["sample"] = f"the first {k} simulations' samples of {pt['net'].name}"
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "sims/s",
@@ -562,6 +603,8 @@ def main():
             line["e2e"] = e2e
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if io is not None:
+            line["io"] = io
         print(json.dumps(line), flush=True)
     for pt in parts:
         del pt["graph"]

@@ -203,3 +203,15 @@ def test_binary_samples_roundtrip(tmp_path, with_cs):
         ctl.read_samples_binary(str(tmp_path / "text"))
     with pytest.raises(ctl.CtlError):
         m.write_samples_binary(str(tmp_path / "no_such_dir" / "x"), samples)
+
+
+def test_bench_io_timing_reports_both_writers():
+    import bench
+    net = inputs.schlogl(6, samples=5, t_end=1.0)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    samples = np.arange(6 * 5 * m.s_out, dtype=np.uint32).reshape(6, 5, m.s_out)
+    io = bench.io_timing(m, samples, threads=2)
+    assert io["sample_sims"] == 6 and io["threads"] == 2
+    assert io["text_s_per_sim"] > 0 and io["binary_s_per_sim"] > 0
+    assert io["binary_bytes_per_sim"] > 5 * m.s_out * 4 - 1
+    assert io["text_bytes_per_sim"] > 0
