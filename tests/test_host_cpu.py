@@ -203,6 +203,10 @@ def test_binary_samples_roundtrip(tmp_path, with_cs):
         ctl.read_samples_binary(str(tmp_path / "text"))
     with pytest.raises(ctl.CtlError):
         m.write_samples_binary(str(tmp_path / "no_such_dir" / "x"), samples)
+    empty = np.zeros((0, 9, so), np.uint32)
+    m.write_samples_binary(str(tmp_path / "empty.ctlbin"), empty)
+    e = ctl.read_samples_binary(str(tmp_path / "empty.ctlbin"))
+    assert e["samples"].shape == (0, 9, so) and np.array_equal(e["t"], d["t"])
 
 
 def test_bench_io_timing_reports_both_writers():
