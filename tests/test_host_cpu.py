@@ -8,6 +8,7 @@ the CLI's early exits keep the reference's exit codes.  No GPU calls."""
 import os
 import re
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -219,3 +220,29 @@ def test_bench_io_timing_reports_both_writers():
     assert io["text_s_per_sim"] > 0 and io["binary_s_per_sim"] > 0
     assert io["binary_bytes_per_sim"] > 5 * m.s_out * 4 - 1
     assert io["text_bytes_per_sim"] > 0
+
+
+def _bench(*args, env_extra=None):
+    env = dict(os.environ, **(env_extra or {}))
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], capture_output=True,
+                          text=True, env=env, timeout=600, cwd=ROOT)
+
+
+def test_bench_reference_arm_line():
+    """`bench.py --impl reference` times the CPU restatement on the host
+    cores and prints one JSON line in the contract's shape; under torchrun
+    only rank 0 works and prints."""
+    import json
+    p = _bench("--impl", "reference", "--config", "1", "--steps", "1", "--warmup", "0")
+    assert p.returncode == 0, p.stderr
+    lines = [x for x in p.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "sims/s" and d["value"] > 0
+    assert d["higher_is_better"] is True and d["n_gpus"] == 1
+    assert d["e2e"] == {"value": d["value"], "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    p1 = _bench("--impl", "reference", "--config", "1", "--steps", "1", "--warmup", "0",
+                env_extra={"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
+    assert p1.returncode == 0 and not [x for x in p1.stdout.splitlines() if x.startswith("{")]
