@@ -90,7 +90,8 @@ typedef struct {
     int32_t threads;      /* threads per block; 0 = autotune                           */
     int32_t uniform_rates;/* 1: every row of c equals row 0 (one shared copy per block);
                              ctl_run detects this itself, device calls take it as given */
-    int32_t ssa_budget;   /* SSA steps per simulation and scheduling round (0 = 16)    */
+    int32_t ssa_budget;   /* SSA steps per simulation and scheduling round (0 = 16; 8
+                             when the batch fits in one wave of resident simulations) */
     int32_t dec_budget;   /* leap decisions per simulation and round (0 = 1; 2 for
                              groups of more than 32 lanes)                            */
     int32_t min_blocks;   /* register budget: kernel variant compiled for this many resident
