@@ -19,7 +19,9 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libctl_oracle.so")
+# CTL_ORACLE_LIB selects another build of the same source (the sanitizer
+# test loads one compiled with -fsanitize=address,undefined).
+LIB_PATH = os.environ.get("CTL_ORACLE_LIB") or os.path.join(HERE, "libctl_oracle.so")
 
 # Quirk switches (0 = reference behaviour); must match ctl_oracle.h.
 FORCE_SSA = 1 << 0
