@@ -40,7 +40,7 @@ EXPORTS = [
     "ctl_status_str", "ctl_last_error", "ctl_model_load", "ctl_model_create", "ctl_model_free",
     "ctl_model_dims_get", "ctl_model_hor", "ctl_rows_load", "ctl_run_cfg_default", "ctl_run",
     "ctl_run_device", "ctl_run_device_noalloc", "ctl_launch_query", "ctl_autotune", "ctl_graph_create", "ctl_graph_launch", "ctl_graph_free",
-    "ctl_write_dynamics", "ctl_print_dynamics", "ctl_write_samples_binary", "ctl_target_load", "ctl_target_free",
+    "ctl_write_dynamics", "ctl_print_dynamics", "ctl_write_samples_binary", "ctl_write_run_report", "ctl_target_load", "ctl_target_free",
     "ctl_target_dims", "ctl_fitness", "ctl_fitness_device", "ctl_mlp_gemm", "ctl_mlp_nll_grad", "ctl_mlp_colsum",
     "ctl_mlp_adam", "ctl_mlp_pack_bytes", "ctl_mlp_pack", "ctl_mlp_screen", "ctl_run_device_sums",
     "ctl_fitness_sums_device", "ctl_fitness_run",
@@ -116,6 +116,7 @@ def lib():
         L.ctl_write_dynamics.argtypes = [P, C.c_char_p, C.c_uint32, P, C.c_uint32, C.c_int32]
         L.ctl_print_dynamics.argtypes = [P, C.c_uint32, P]
         L.ctl_write_samples_binary.argtypes = [P, C.c_char_p, C.c_uint32, P, C.c_uint32]
+        L.ctl_write_run_report.argtypes = [P, C.c_char_p, C.c_uint32, P, C.c_double, P]
         L.ctl_target_load.argtypes = [C.c_char_p, P, C.c_uint32, C.c_uint32, C.POINTER(P)]
         L.ctl_target_free.argtypes = [P]
         L.ctl_target_free.restype = None
@@ -246,6 +247,16 @@ class Model:
         samples = np.ascontiguousarray(samples, dtype=np.uint32)
         _check(lib().ctl_write_dynamics(self._h, os.fsencode(path_prefix), samples.shape[0],
                                         _p(samples), first_id, threads), "ctl_write_dynamics")
+
+    def write_run_report(self, path: str, info, seconds: float, launch: "LaunchInfo | None" = None):
+        """JSON run report for the records `info` of a run that took
+        `seconds` (ctl_write_run_report)."""
+        info = np.ascontiguousarray(info)
+        if info.dtype != INFO_DTYPE:
+            info = info.view(INFO_DTYPE).reshape(-1)
+        _check(lib().ctl_write_run_report(self._h, os.fsencode(path), info.shape[0], _p(info), float(seconds),
+                                          C.byref(launch) if launch is not None else None),
+               "ctl_write_run_report")
 
     def write_samples_binary(self, path: str, samples, first_id=0):
         """The whole batch in one binary file (ctl_write_samples_binary);

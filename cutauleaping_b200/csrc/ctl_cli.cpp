@@ -20,6 +20,8 @@
 //   CTL_BINARY_OUTPUT=1  one binary file <output_folder><prefix>.ctlbin
 //                  (ctl_write_samples_binary) instead of a text file per
 //                  simulation
+//   CTL_REPORT=<path>  a JSON run report (ctl_write_run_report): rates,
+//                  step counts, per-status counts, launch shape
 #include <sys/stat.h>
 #include <sys/types.h>
 
@@ -183,8 +185,15 @@ int main(int argc, const char* argv[]) {
     clock_gettime(CLOCK_MONOTONIC, &t1);
     if (st != CTL_OK && st != CTL_ERR_STEP_LIMIT) return exit_code(st, just_fitness ? "fitness" : "run");
     if (st == CTL_ERR_STEP_LIMIT) fprintf(stderr, "WARNING: %s\n", ctl_last_error());
-    if (verbose)
-        printf(" * RUNNING TIME: %f seconds.\n", (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec));
+    const double run_s = (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
+    if (verbose) printf(" * RUNNING TIME: %f seconds.\n", run_s);
+    if (const char* rep = getenv("CTL_REPORT")) {
+        ctl_launch_info li;
+        const bool have = ctl_launch_query(model, &cfg, N, &li) == CTL_OK;
+        if (ctl_write_run_report(model, rep, N, info.data(), run_s > 0.0 ? run_s : 1e-9, have ? &li : nullptr) !=
+            CTL_OK)
+            fprintf(stderr, "WARNING: %s\n", ctl_last_error());
+    }
 
     std::string dumpfile = out_dir + prefix;
     if (!just_fitness) {

@@ -460,6 +460,49 @@ extern "C" ctl_status ctl_write_samples_binary(const ctl_model* m, const char* p
     return CTL_OK;
 }
 
+extern "C" ctl_status ctl_write_run_report(const ctl_model* m, const char* path, uint32_t n,
+                                           const ctl_sim_info* info, double seconds,
+                                           const ctl_launch_info* launch) {
+    if (!m || !path || (!info && n)) return fail(CTL_ERR_ARG, "null argument");
+    if (!(seconds > 0.0) || !std::isfinite(seconds)) return fail(CTL_ERR_ARG, "seconds must be positive");
+    const HostTables& t = m->t;
+    unsigned long long firings = 0, steps = 0, leaps = 0, ssa = 0, rej = 0, st[4] = {0, 0, 0, 0}, other = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        firings += info[i].firings;
+        steps += info[i].steps;
+        leaps += info[i].leaps;
+        ssa += info[i].ssa_steps;
+        rej += info[i].rejections;
+        if (info[i].status < 4) st[info[i].status]++;
+        else other++;
+    }
+    // X0 (4S) + c (4R) + samples (4 ns s_out) + the 40-byte record
+    const double bytes = 4.0 * t.S + 4.0 * t.R + 4.0 * t.ns * t.s_out + (double)sizeof(ctl_sim_info);
+    std::ostringstream o;
+    o.precision(17);
+    o << "{\"simulations\": " << n << ", \"seconds\": " << seconds
+      << ", \"sims_per_s\": " << n / seconds << ", \"firings\": " << firings
+      << ", \"firings_per_s\": " << (double)firings / seconds << ", \"steps\": " << steps
+      << ", \"leaps\": " << leaps << ", \"ssa_steps\": " << ssa << ", \"rejections\": " << rej
+      << ", \"status\": {\"ok\": " << st[CTL_SIM_OK] << ", \"step_limit\": " << st[CTL_SIM_STEP_LIMIT]
+      << ", \"overflow\": " << st[CTL_SIM_OVERFLOW] << ", \"attempt_limit\": " << st[CTL_SIM_ATTEMPT_LIMIT]
+      << ", \"other\": " << other << "}, \"species\": " << t.S << ", \"reactions\": " << t.R
+      << ", \"instants\": " << t.ns << ", \"sampled_species\": " << t.s_out
+      << ", \"hbm_bytes_per_sim\": " << bytes << ", \"hbm_gb_per_s\": " << bytes * n / seconds / 1e9;
+    if (launch)
+        o << ", \"launch\": {\"group\": " << launch->group << ", \"threads\": " << launch->threads
+          << ", \"blocks\": " << launch->blocks << ", \"min_blocks\": " << launch->min_blocks
+          << ", \"sched\": " << launch->sched << ", \"ssa_budget\": " << launch->ssa_budget
+          << ", \"dec_budget\": " << launch->dec_budget << "}";
+    o << "}\n";
+    const std::string js = o.str();
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return fail(CTL_ERR_IO, std::string("cannot write ") + path);
+    const bool ok = std::fwrite(js.data(), 1, js.size(), fp) == js.size();
+    if (std::fclose(fp) != 0 || !ok) return fail(CTL_ERR_IO, std::string("cannot write ") + path);
+    return CTL_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Fitness targets (read_time_series, tau.cu:1056-1261)
 // ---------------------------------------------------------------------------

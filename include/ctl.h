@@ -208,6 +208,14 @@ ctl_status ctl_print_dynamics(const ctl_model* m, uint32_t n, const uint32_t* sa
  * samples[n][ns][s_out] exactly as ctl_run returns them. */
 ctl_status ctl_write_samples_binary(const ctl_model* m, const char* path, uint32_t n,
                                     const uint32_t* samples, uint32_t first_id);
+/* Structured run report (the reference prints only "RUNNING TIME" under
+ * verbose, kernel.cu:347): one JSON object with the batch size, the wall
+ * seconds given, simulations and reaction firings per second, summed
+ * steps / leaps / SSA steps / rejections, per-status counts, the algorithmic
+ * HBM bytes per simulation and their rate, and the launch shape when
+ * `launch` is not null.  Host code only. */
+ctl_status ctl_write_run_report(const ctl_model* m, const char* path, uint32_t n, const ctl_sim_info* info,
+                                double seconds, const ctl_launch_info* launch);
 
 /* ---- fitness ------------------------------------------------------------- */
 /* read_time_series (tau.cu:1056-1261): ts_rep, p_rep, ts_numtgt, tts_vector,

@@ -5,7 +5,7 @@ verbose` (kernel.cu:74-436) must write the per-simulation files of
 WriteDynamics2 (2phase_n-tau-leaping.cu:3431-3469) with the oracle's samples,
 honour `offset` (rows and random streams of a larger run), force SSA, print
 dynamics to stdout with verbose = 2, write one binary sample file with
-CTL_BINARY_OUTPUT=1, and print calculateFitness
+CTL_BINARY_OUTPUT=1, write a JSON run report with CTL_REPORT, and print calculateFitness
 (3324-3408) values in fitness mode 2 -- checked against a numpy restatement.
 """
 import os
@@ -59,6 +59,21 @@ def test_cli_binary_output_matches_oracle(folder, tmp_path):
     assert np.array_equal(np.asarray(d["samples"]), ref)
     assert np.array_equal(d["t"], np.asarray(net.tvec, np.float64))
     assert sorted(os.listdir(tmp_path / "ob")) == ["pref.ctlbin"]
+
+
+def test_cli_run_report(folder, tmp_path):
+    """CTL_REPORT=<path>: a JSON run report whose sums match the oracle's
+    per-simulation records."""
+    import json
+    path, net = folder
+    rep = tmp_path / "report.json"
+    p = _cli([path, 8, 2, 0, 8, tmp_path / "or", "pref", 0, 0, 0], {"CTL_REPORT": str(rep)})
+    assert p.returncode == 0, p.stderr
+    _, info = oracle_model(net, seed=5).run(net.X0[8:24], net.c[8:24].astype(np.float32), sim_base=8)
+    r = json.loads(rep.read_text())
+    assert r["simulations"] == 16 and r["status"]["ok"] == 16 and r["seconds"] > 0
+    assert r["firings"] == int(info["firings"].sum()) and r["steps"] == int(info["steps"].sum())
+    assert r["launch"]["group"] >= 1 and r["launch"]["threads"] >= 32
 
 
 def test_cli_stdout_dynamics(folder, tmp_path):

@@ -246,3 +246,34 @@ def test_bench_reference_arm_line():
     p1 = _bench("--impl", "reference", "--config", "1", "--steps", "1", "--warmup", "0",
                 env_extra={"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert p1.returncode == 0 and not [x for x in p1.stdout.splitlines() if x.startswith("{")]
+
+
+def test_run_report_json(tmp_path):
+    """ctl_write_run_report: rates, sums, per-status counts and launch shape
+    as one JSON object (host code; records made up here)."""
+    import json
+    net = inputs.schlogl(4, samples=10, t_end=1.0)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    info = np.zeros(4, dtype=ctl.INFO_DTYPE)
+    info["firings"] = [10, 20, 30, 40]
+    info["steps"] = [5, 6, 7, 8]
+    info["leaps"] = [1, 2, 3, 4]
+    info["ssa_steps"] = [4, 4, 4, 4]
+    info["rejections"] = [0, 1, 0, 1]
+    info["status"] = [ctl.SIM_OK, ctl.SIM_OK, ctl.SIM_STEP_LIMIT, 7]
+    li = ctl.LaunchInfo()
+    li.group, li.threads, li.blocks, li.min_blocks, li.sched, li.ssa_budget, li.dec_budget = 4, 96, 2, 2, 1, 8, 1
+    path = str(tmp_path / "report.json")
+    m.write_run_report(path, info, 0.5, li)
+    r = json.load(open(path))
+    assert r["simulations"] == 4 and r["seconds"] == 0.5 and r["sims_per_s"] == 8.0
+    assert r["firings"] == 100 and r["firings_per_s"] == 200.0
+    assert (r["steps"], r["leaps"], r["ssa_steps"], r["rejections"]) == (26, 10, 16, 2)
+    assert r["status"] == {"ok": 2, "step_limit": 1, "overflow": 0, "attempt_limit": 0, "other": 1}
+    assert r["hbm_bytes_per_sim"] == 4 * m.S + 4 * m.R + 4 * m.ns * m.s_out + 40
+    assert r["launch"] == {"group": 4, "threads": 96, "blocks": 2, "min_blocks": 2, "sched": 1,
+                           "ssa_budget": 8, "dec_budget": 1}
+    m.write_run_report(str(tmp_path / "nolaunch.json"), info, 2.0)
+    assert "launch" not in json.load(open(tmp_path / "nolaunch.json"))
+    with pytest.raises(ctl.CtlError):
+        m.write_run_report(str(tmp_path / "bad.json"), info, 0.0)
