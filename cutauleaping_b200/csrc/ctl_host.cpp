@@ -19,6 +19,7 @@
 #include <iostream>
 #include <sstream>
 #include <memory>
+#include <new>
 #include <thread>
 
 #include "ctl_internal.h"
@@ -176,11 +177,12 @@ static bool parse_double(const std::string& tok, double& v) {
     v = std::strtod(p, &end);
     return end != p;
 }
-static bool parse_long(const std::string& tok, long& v) {
+static bool parse_long(const std::string& tok, long& v) {  // out-of-range values are errors
     const char* p = tok.c_str();
     char* end = nullptr;
+    errno = 0;
     v = std::strtol(p, &end, 10);
-    return end != p;
+    return end != p && errno != ERANGE;
 }
 
 }  // namespace ctl
@@ -208,7 +210,7 @@ extern "C" const char* ctl_status_str(ctl_status s) {
 
 extern "C" const char* ctl_last_error(void) { return ctl::g_last_error.c_str(); }
 
-extern "C" ctl_status ctl_model_create(int32_t S, int32_t R, const int32_t* left,
+static ctl_status model_create_impl(int32_t S, int32_t R, const int32_t* left,
                                        const int32_t* right, const int32_t* feed, int32_t ns,
                                        const double* tvec, int32_t s_out, const int32_t* cs,
                                        ctl_model** out) {
@@ -222,7 +224,7 @@ extern "C" ctl_status ctl_model_create(int32_t S, int32_t R, const int32_t* left
     return CTL_OK;
 }
 
-extern "C" ctl_status ctl_model_load(const char* folder, ctl_model** out) {
+static ctl_status model_load_impl(const char* folder, ctl_model** out) {
     if (!folder || !out) return fail(CTL_ERR_ARG, "null argument");
     *out = nullptr;
     std::string f(folder);
@@ -308,7 +310,7 @@ extern "C" ctl_status ctl_model_hor(const ctl_model* m, uint8_t* hor, uint8_t* h
     return CTL_OK;
 }
 
-extern "C" ctl_status ctl_rows_load(const char* folder, int32_t S, int32_t R, uint32_t offset,
+static ctl_status rows_load_impl(const char* folder, int32_t S, int32_t R, uint32_t offset,
                                     uint32_t n, int32_t* X0, float* c) {
     if (!folder || !X0 || !c) return fail(CTL_ERR_ARG, "null argument");
     std::string f(folder);
@@ -376,7 +378,7 @@ static void append_sim(std::string& buf, const HostTables& t, const std::vector<
     }
 }
 
-extern "C" ctl_status ctl_write_dynamics(const ctl_model* m, const char* path_prefix, uint32_t n,
+static ctl_status write_dynamics_impl(const ctl_model* m, const char* path_prefix, uint32_t n,
                                          const uint32_t* samples, uint32_t first_id, int32_t nthreads) {
     if (!m || !path_prefix || (!samples && n)) return fail(CTL_ERR_ARG, "null argument");
     const HostTables& t = m->t;
@@ -388,32 +390,42 @@ extern "C" ctl_status ctl_write_dynamics(const ctl_model* m, const char* path_pr
     std::atomic<int> err(0);
     std::string err_path;
     std::mutex err_mu;
+    std::atomic<int> oom(0);
     auto work = [&]() {
-        std::string buf;
-        for (;;) {
-            uint32_t i = next.fetch_add(1);
-            if (i >= n) break;
-            buf.clear();
-            append_sim(buf, t, ts, samples + (size_t)i * t.ns * t.s_out);
-            std::string name = prefix + "_" + std::to_string((unsigned long long)first_id + i);
-            FILE* fp = std::fopen(name.c_str(), "wb");
-            if (!fp || std::fwrite(buf.data(), 1, buf.size(), fp) != buf.size()) {
-                std::lock_guard<std::mutex> lk(err_mu);
-                err = 1;
-                err_path = name;
+        try {  // nothing may escape a worker thread
+            std::string buf;
+            for (;;) {
+                uint32_t i = next.fetch_add(1);
+                if (i >= n) break;
+                buf.clear();
+                append_sim(buf, t, ts, samples + (size_t)i * t.ns * t.s_out);
+                std::string name = prefix + "_" + std::to_string((unsigned long long)first_id + i);
+                FILE* fp = std::fopen(name.c_str(), "wb");
+                if (!fp || std::fwrite(buf.data(), 1, buf.size(), fp) != buf.size()) {
+                    std::lock_guard<std::mutex> lk(err_mu);
+                    err = 1;
+                    err_path = name;
+                }
+                if (fp) std::fclose(fp);
             }
-            if (fp) std::fclose(fp);
+        } catch (...) {
+            oom = 1;
+            next = n;  // the other workers stop too
         }
     };
     std::vector<std::thread> pool;
-    for (int k = 1; k < nthreads; k++) pool.emplace_back(work);
+    try {
+        for (int k = 1; k < nthreads; k++) pool.emplace_back(work);
+    } catch (...) {  // fewer threads than asked: the ones started and this one finish the work
+    }
     work();
     for (auto& th : pool) th.join();
+    if (oom) return fail(CTL_ERR_OOM, "ctl_write_dynamics: host allocation failed");
     if (err) return fail(CTL_ERR_IO, "cannot write " + err_path);
     return CTL_OK;
 }
 
-extern "C" ctl_status ctl_print_dynamics(const ctl_model* m, uint32_t n, const uint32_t* samples) {
+static ctl_status print_dynamics_impl(const ctl_model* m, uint32_t n, const uint32_t* samples) {
     if (!m || (!samples && n)) return fail(CTL_ERR_ARG, "null argument");
     const HostTables& t = m->t;
     std::vector<std::string> ts = time_strings(t);
@@ -428,7 +440,7 @@ extern "C" ctl_status ctl_print_dynamics(const ctl_model* m, uint32_t n, const u
     return CTL_OK;
 }
 
-extern "C" ctl_status ctl_write_samples_binary(const ctl_model* m, const char* path, uint32_t n,
+static ctl_status write_samples_binary_impl(const ctl_model* m, const char* path, uint32_t n,
                                                const uint32_t* samples, uint32_t first_id) {
     if (!m || !path || (!samples && n)) return fail(CTL_ERR_ARG, "null argument");
     const HostTables& t = m->t;
@@ -460,7 +472,7 @@ extern "C" ctl_status ctl_write_samples_binary(const ctl_model* m, const char* p
     return CTL_OK;
 }
 
-extern "C" ctl_status ctl_write_run_report(const ctl_model* m, const char* path, uint32_t n,
+static ctl_status write_run_report_impl(const ctl_model* m, const char* path, uint32_t n,
                                            const ctl_sim_info* info, double seconds,
                                            const ctl_launch_info* launch) {
     if (!m || !path || (!info && n)) return fail(CTL_ERR_ARG, "null argument");
@@ -507,7 +519,7 @@ extern "C" ctl_status ctl_write_run_report(const ctl_model* m, const char* path,
 // Fitness targets (read_time_series, tau.cu:1056-1261)
 // ---------------------------------------------------------------------------
 
-extern "C" ctl_status ctl_target_load(const char* folder, const ctl_model* m, uint32_t threads,
+static ctl_status target_load_impl(const char* folder, const ctl_model* m, uint32_t threads,
                                       uint32_t blocks, ctl_target** out) {
     if (!folder || !m || !out) return fail(CTL_ERR_ARG, "null argument");
     *out = nullptr;
@@ -556,7 +568,11 @@ extern "C" ctl_status ctl_target_load(const char* folder, const ctl_model* m, ui
     // ts_matrix: one row per sample, first column the instant, then
     // experiments x repetitions x target_quantities counts.
     if (!read_lines(f + "/ts_matrix", lines)) return fail(CTL_ERR_IO, "WARNING: cannot open ts file (fitness unavailable)");
-    uint32_t cols = t->experiments * t->repetitions * t->target_quantities;
+    const uint64_t cols64 = (uint64_t)t->experiments * t->repetitions * t->target_quantities;
+    if (cols64 > ((uint64_t)1 << 24) || cols64 * t->ns > ((uint64_t)1 << 31))
+        return fail(CTL_ERR_SHAPE, "ts_matrix: " + std::to_string(cols64) +
+                                       " columns per instant (experiments x repetitions x quantities) is too large");
+    const uint32_t cols = (uint32_t)cols64;
     t->series.assign((size_t)t->ns * cols, 0);
     uint32_t row = 0;
     for (auto& l : lines) {
@@ -573,6 +589,70 @@ extern "C" ctl_status ctl_target_load(const char* folder, const ctl_model* m, ui
     }
     *out = t.release();
     return CTL_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// C ABI entry points of the host code: no C++ exception leaves the library
+// (a failed host allocation becomes CTL_ERR_OOM, anything else CTL_ERR_ARG,
+// with the message in ctl_last_error).
+// ---------------------------------------------------------------------------
+
+template <class F>
+static ctl_status guarded(const char* what, F&& f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return fail(CTL_ERR_OOM, std::string(what) + ": host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(CTL_ERR_ARG, std::string(what) + ": " + e.what());
+    } catch (...) {
+        return fail(CTL_ERR_ARG, std::string(what) + ": unexpected failure");
+    }
+}
+
+extern "C" ctl_status ctl_model_create(int32_t S, int32_t R, const int32_t* left, const int32_t* right,
+                                       const int32_t* feed, int32_t ns, const double* tvec, int32_t s_out,
+                                       const int32_t* cs, ctl_model** out) {
+    return guarded("ctl_model_create",
+                   [&] { return model_create_impl(S, R, left, right, feed, ns, tvec, s_out, cs, out); });
+}
+
+extern "C" ctl_status ctl_model_load(const char* folder, ctl_model** out) {
+    return guarded("ctl_model_load", [&] { return model_load_impl(folder, out); });
+}
+
+extern "C" ctl_status ctl_rows_load(const char* folder, int32_t S, int32_t R, uint32_t offset, uint32_t n,
+                                    int32_t* X0, float* c) {
+    return guarded("ctl_rows_load", [&] { return rows_load_impl(folder, S, R, offset, n, X0, c); });
+}
+
+extern "C" ctl_status ctl_write_dynamics(const ctl_model* m, const char* path_prefix, uint32_t n,
+                                         const uint32_t* samples, uint32_t first_id, int32_t nthreads) {
+    return guarded("ctl_write_dynamics",
+                   [&] { return write_dynamics_impl(m, path_prefix, n, samples, first_id, nthreads); });
+}
+
+extern "C" ctl_status ctl_print_dynamics(const ctl_model* m, uint32_t n, const uint32_t* samples) {
+    return guarded("ctl_print_dynamics", [&] { return print_dynamics_impl(m, n, samples); });
+}
+
+extern "C" ctl_status ctl_write_samples_binary(const ctl_model* m, const char* path, uint32_t n,
+                                               const uint32_t* samples, uint32_t first_id) {
+    return guarded("ctl_write_samples_binary",
+                   [&] { return write_samples_binary_impl(m, path, n, samples, first_id); });
+}
+
+extern "C" ctl_status ctl_write_run_report(const ctl_model* m, const char* path, uint32_t n,
+                                           const ctl_sim_info* info, double seconds,
+                                           const ctl_launch_info* launch) {
+    return guarded("ctl_write_run_report",
+                   [&] { return write_run_report_impl(m, path, n, info, seconds, launch); });
+}
+
+extern "C" ctl_status ctl_target_load(const char* folder, const ctl_model* m, uint32_t threads,
+                                      uint32_t blocks, ctl_target** out) {
+    return guarded("ctl_target_load", [&] { return target_load_impl(folder, m, threads, blocks, out); });
 }
 
 extern "C" void ctl_target_free(ctl_target* t) { delete t; }
