@@ -91,7 +91,7 @@ def _math_names(kl) -> list:
 def load(path: str, *, reference_feeds: bool = False) -> SbmlModel:
     try:
         root = ET.parse(path).getroot()
-    except (ET.ParseError, OSError) as e:
+    except (ET.ParseError, OSError, LookupError, UnicodeError, ValueError) as e:
         raise SbmlError(f"cannot read SBML file {path}: {e}")
     model = _child(root, "model")
     if model is None:
@@ -109,7 +109,10 @@ def load(path: str, *, reference_feeds: bool = False) -> SbmlModel:
         if amount is None or math.isnan(_float(amount, sid)):
             amount = sp.get("initialConcentration", "0")
         held = sp.get("boundaryCondition") == "true" or sp.get("constant") == "true"
-        species.append((sid, label, _float(amount, f"initial amount of {sid}"), held))
+        x0 = _float(amount, f"initial amount of {sid}")
+        if not math.isfinite(x0):
+            raise SbmlError(f"initial amount of {sid} is not finite")
+        species.append((sid, label, x0, held))
     if not species:
         raise SbmlError("the model has no species")
     index = {sid: i for i, (sid, _, _, _) in enumerate(species)}
@@ -127,8 +130,8 @@ def load(path: str, *, reference_feeds: bool = False) -> SbmlModel:
                 if sp not in index:
                     raise SbmlError(f"reaction {rid}: unknown species {sp}")
                 st = _float(ref.get("stoichiometry", "1"), f"stoichiometry in {rid}")
-                if st != int(st) or st < 0:
-                    raise SbmlError(f"reaction {rid}: stoichiometry must be a non-negative integer")
+                if not (0 <= st <= 127) or st != int(st):
+                    raise SbmlError(f"reaction {rid}: stoichiometry must be an integer in [0, 127]")
                 v[index[sp]] += int(st)
             return v
         lv, rv = side("listOfReactants"), side("listOfProducts")
@@ -147,6 +150,8 @@ def load(path: str, *, reference_feeds: bool = False) -> SbmlModel:
             if not named:
                 raise SbmlError(f"reaction {rid}: no kinetic parameter found")
             consts = [params[n] for n in named]
+        if not all(math.isfinite(k) and k >= 0 for k in consts):
+            raise SbmlError(f"reaction {rid}: rate constants must be finite and >= 0")
         reverse = rx.get("reversible") == "true" or len(consts) == 2
         if len(consts) > 2 or (reverse and len(consts) != 2) or len(consts) == 0:
             raise SbmlError(f"reaction {rid}: expected one rate constant (two if reversible), "

@@ -64,3 +64,38 @@ def test_command_line(tmp_path, capsys):
     assert sbml.main([os.path.join(GOLDEN, "dimer_l3.xml"), str(tmp_path / "o"), "--sims", "3"]) == 0
     assert open(tmp_path / "o" / "MX_0").read() == "400\t0\n" * 3
     assert sbml.main([str(tmp_path / "missing.xml"), str(tmp_path / "o2")]) == 2
+
+
+def test_mutated_sbml_raises_only_sbml_errors(tmp_path):
+    """Seeded random damage to the two fixtures -- cut, inserted and
+    truncated text, odd attribute values (negative, huge, non-numeric,
+    infinite), unknown XML encodings -- either imports or raises SbmlError."""
+    import random
+    srcs = [open(os.path.join(GOLDEN, n)).read() for n in ("schlogl_l2.xml", "dimer_l3.xml")]
+    tokens = ["<", ">", "/", "\"", "=", " ", "x", "-1", "1e400", "nan", "2.5", "true", "</model>",
+              "<species id=\"q\"/>", "reversible=\"true\"", "stoichiometry=\"-3\"", "stoichiometry=\"1.5\"",
+              "<ci> k </ci>", "&amp;", "&bad;"]
+    rng = random.Random(5)
+    path = str(tmp_path / "m.xml")
+    for _ in range(800):
+        d = rng.choice(srcs)
+        for _ in range(rng.randint(1, 5)):
+            i, op = rng.randrange(len(d) + 1), rng.randrange(4)
+            if op == 0:
+                d = d[:i] + d[i + rng.randint(1, 40):]
+            elif op == 1:
+                d = d[:i] + rng.choice(tokens) + d[i:]
+            elif op == 2:
+                a = d.find('"', i)
+                b = d.find('"', a + 1)
+                if a >= 0 and b > a:
+                    d = d[:a + 1] + rng.choice(["", "0", "-5", "abc", "1e308", "inf", "3", "UTFx-8"]) + d[b:]
+            else:
+                d = d[:i]
+        with open(path, "w") as f:
+            f.write(d)
+        try:
+            m = sbml.load(path)
+            sbml.write_folder(m, str(tmp_path / "out"), sims=2, t_end=1.0, samples=3)
+        except sbml.SbmlError:
+            pass
