@@ -32,6 +32,7 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -96,15 +97,37 @@ static unsigned long long env_u(const char* k, unsigned long long d) {
     return v ? strtoull(v, nullptr, 0) : d;
 }
 
-int main(int argc, const char* argv[]) {
+// threads / blocks / offset as the reference reads them (atoi), but a
+// negative value is an error instead of a huge unsigned one.
+static bool count_arg(const char* s, unsigned& v) {
+    const long x = atol(s);
+    if (x < 0 || x > 0xffffffffL) return false;
+    v = (unsigned)x;
+    return true;
+}
+
+// Rows of MX_0 (lines, as the library counts them), to reject a batch that
+// cannot fit before allocating host buffers for it; -1 if unreadable.
+static long long mx0_rows(const char* folder) {
+    std::ifstream in((std::string(folder) + "/MX_0").c_str());
+    if (!in.is_open()) return -1;
+    long long rows = 0;
+    for (std::string line; std::getline(in, line);) rows++;
+    return rows;
+}
+
+static int run_cli(int argc, const char* argv[]) {
     if (argc < 6) usage_exit();
     const bool verbose = argc > 10 && std::string(argv[10]) == "1";
     const bool stdout_dyn = argc > 10 && std::string(argv[10]) == "2";
     const char* folder = argv[1];
-    const unsigned threads = (unsigned)atoi(argv[2]);
-    const unsigned blocks = (unsigned)atoi(argv[3]);
+    unsigned threads = 0, blocks = 0, offset = 0;
     const int gpu = atoi(argv[4]);
-    const unsigned offset = (unsigned)atoi(argv[5]);
+    if (!count_arg(argv[2], threads) || !count_arg(argv[3], blocks) || !count_arg(argv[5], offset) ||
+        (unsigned long long)threads * blocks > 0xffffffffull) {
+        fprintf(stderr, "ERROR: threads, blocks and offset must be non-negative and threads*blocks < 2^32\n");
+        return -1;
+    }
     const unsigned N = threads * blocks;
     if (verbose) {
         printf(" * Required %d threads per block using %d blocks", threads, blocks);
@@ -138,6 +161,11 @@ int main(int argc, const char* argv[]) {
     }
     ctl_model_dims dims;
     ctl_model_dims_get(model, &dims);
+    const long long rows = mx0_rows(folder);
+    if (rows >= 0 && (long long)offset + N > rows) {  // the library's message and exit code, before any allocation
+        fprintf(stderr, "ERROR: input files rows (%lld) and requested threads (%u) do not fit\n", rows, N);
+        return -4;
+    }
     std::vector<int32_t> X0((size_t)N * dims.S);
     std::vector<float> c((size_t)N * dims.R);
     st = ctl_rows_load(folder, dims.S, dims.R, offset, N, X0.data(), c.data());
@@ -235,4 +263,13 @@ int main(int argc, const char* argv[]) {
     }
     ctl_model_free(model);
     return 0;
+}
+
+int main(int argc, const char* argv[]) {
+    try {
+        return run_cli(argc, argv);
+    } catch (const std::bad_alloc&) {
+        fprintf(stderr, "ERROR: out of host memory\n");
+        return -3;
+    }
 }

@@ -160,6 +160,13 @@ def test_cli_usage_and_early_exit_codes(tmp_path):
     folder2 = _folder(tmp_path / "x", MX_0=None)
     p = _cli(folder2, 2, 2, 0, 0, tmp_path / "out", "pref", 0, 0, 0)
     assert p.returncode == 256 - 6
+    # negative counts and threads*blocks beyond 32 bits are refused before any work
+    for args in ((-4, 4, 0), (4, -4, 0), (4, 4, -1), (70000, 70000, 0)):
+        p = _cli(folder, args[0], args[1], 0, args[2], tmp_path / "out", "pref", 0, 0, 0)
+        assert p.returncode == 255 and "threads*blocks" in p.stderr, (args, p.stderr)
+    # a batch far beyond the rows of MX_0 is refused before its buffers are allocated
+    p = _cli(folder, 65536, 65535, 0, 0, tmp_path / "out", "pref", 0, 0, 0)
+    assert p.returncode == 256 - 4 and "do not fit" in p.stderr
 
 
 @pytest.mark.parametrize("kw", [{"min_blocks": 1}, {"min_blocks": 5}, {"ssa_steps": 0}, {"sched": 3},
