@@ -44,8 +44,14 @@ ctl_status build_tables(int S, int R, const int32_t* left, const int32_t* right,
                         const int32_t* cs, HostTables& t) {
     if (S <= 0 || R <= 0) return fail(CTL_ERR_SHAPE, "model needs at least one species and one reaction");
     if (S >= (1 << 24) || R >= (1 << 24)) return fail(CTL_ERR_SHAPE, "more than 2^24 species or reactions");
+    if ((int64_t)S * R > ((int64_t)1 << 28)) return fail(CTL_ERR_SHAPE, "more than 2^28 stoichiometry entries");
     if (ns <= 0) return fail(CTL_ERR_SHAPE, "t_vector holds no sample instants");
     if (!left || !right || !tvec) return fail(CTL_ERR_ARG, "null model array");
+    // A NaN or infinite instant would never be reached (the simulation would
+    // run to its step cap), a negative one never compared: both are errors.
+    for (int i = 0; i < ns; i++)
+        if (!std::isfinite(tvec[i]) || tvec[i] < 0.0)
+            return fail(CTL_ERR_SHAPE, "t_vector: instant " + std::to_string(i) + " is negative or not finite");
     for (int i = 0; i < R * S; i++) {
         if (left[i] < 0 || left[i] > 127 || right[i] < 0 || right[i] > 127)
             return fail(CTL_ERR_SHAPE, "stoichiometric coefficients must lie in [0, 127]");

@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <chrono>
@@ -583,6 +584,28 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     return CTL_OK;
 }
 
+// Host rows given to ctl_run / ctl_fitness_run: counts >= 0 and rate
+// constants finite and >= 0 (row 0 only when the caller declares every row
+// equal).  A NaN or infinite rate makes the propensity sum non-finite, and
+// simulated time then never reaches the next sample instant: the simulation
+// would run to its step cap.
+static ctl_status check_host_rows(const HostTables& t, uint32_t n, const int32_t* X0, const float* c,
+                                  bool uniform) {
+    const size_t nx = (size_t)n * (size_t)t.S;
+    for (size_t i = 0; i < nx; i++)
+        if (X0[i] < 0) {
+            set_error("X0: negative count in row " + std::to_string(i / (size_t)t.S));
+            return CTL_ERR_ARG;
+        }
+    const size_t nc = (uniform ? (size_t)1 : (size_t)n) * (size_t)t.R;
+    for (size_t i = 0; i < nc; i++)
+        if (!(c[i] >= 0.0f) || !std::isfinite(c[i])) {
+            set_error("c: rate constant in row " + std::to_string(i / (size_t)t.R) + " is negative or not finite");
+            return CTL_ERR_ARG;
+        }
+    return CTL_OK;
+}
+
 static ctl_status check_cfg(const ctl_run_cfg* cfg) {
     if (!cfg) {
         set_error("null run configuration");
@@ -693,6 +716,7 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
         return CTL_ERR_ARG;
     }
     const HostTables& t = m->t;
+    if ((st = check_host_rows(t, n, X0, c, cfg->uniform_rates != 0)) != CTL_OK) return st;
     DeviceGuard dg(cfg->device);
     DeviceCopy* d = nullptr;
     if ((st = ensure_device(m, cfg->device, d)) != CTL_OK) return st;
@@ -1125,6 +1149,7 @@ extern "C" ctl_status ctl_fitness_run(ctl_model* m, const ctl_target* t, const c
     const uint32_t N = (uint32_t)N64;
     if ((st = check_sums_shape(N, t->threads, t->p_rep)) != CTL_OK) return st;
     const uint32_t nsets = N / t->p_rep;
+    if ((st = check_host_rows(h, N, X0, c, cfg->uniform_rates != 0)) != CTL_OK) return st;
     DeviceGuard dg(cfg->device);
     DeviceCopy* d = nullptr;
     if ((st = ensure_device(m, cfg->device, d)) != CTL_OK) return st;

@@ -284,3 +284,33 @@ def test_run_report_json(tmp_path):
     assert "launch" not in json.load(open(tmp_path / "nolaunch.json"))
     with pytest.raises(ctl.CtlError):
         m.write_run_report(str(tmp_path / "bad.json"), info, 0.0)
+
+
+@pytest.mark.parametrize("bad", ["nan_rate", "inf_rate", "negative_rate", "negative_count"])
+def test_host_rows_rejected_before_device_work(bad):
+    """ctl_run refuses rows that would make a simulation run to its step cap
+    (non-finite rates) or that are not counts, before touching a device."""
+    net = inputs.schlogl(4, samples=5, t_end=1.0)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    X0 = np.array(net.X0, np.int32)
+    c = np.array(net.c, np.float32)
+    if bad == "nan_rate":
+        c[2, 1] = np.nan
+    elif bad == "inf_rate":
+        c[3, 0] = np.inf
+    elif bad == "negative_rate":
+        c[1, 3] = -1e-3
+    else:
+        X0[2, 0] = -5
+    with pytest.raises(ctl.CtlError) as e:
+        m.run(X0, c, seed=1)
+    assert e.value.status == ctl.ERR_ARG and ("c:" in str(e.value) or "X0:" in str(e.value))
+
+
+def test_model_instants_must_be_finite_and_non_negative():
+    left, right = np.array([[1, 0]], np.int32), np.array([[0, 1]], np.int32)
+    for tv in ([0.5, np.nan], [0.5, np.inf], [-1.0, 0.5]):
+        with pytest.raises(ctl.CtlError) as e:
+            ctl.Model.create(left, right, None, np.array(tv))
+        assert e.value.status == ctl.ERR_SHAPE
+    ctl.Model.create(left, right, None, np.array([0.0, 0.5, 0.2]))  # zero and unsorted instants stay valid
