@@ -145,3 +145,21 @@ def test_oracle_matches_reference_binary(path):
     vz = [stats.var_z(ours_raw[:, i, j], raw[:, i, j]) for i in range(raw.shape[1]) for j in range(raw.shape[2])]
     vz = np.abs(np.array(vz))
     assert vz.max() < 4.5 and (vz > 3).mean() <= 0.05, f"{name}: variance z {np.sort(vz)[-5:]}"
+
+
+@pytest.mark.parametrize("S,R,seed,t_end,samples,extra", [
+    (64, 128, 0, 10.0, 200, {}),                                                   # config 2
+    (32, 64, 3, 10.0, 200, {}),                                                    # config 3, synthetic part
+    (512, 1024, 0, 20.0, 500, {"c_range": (1e-5, 1e-1), "x0_range": (1, 100000)}),  # config 4
+])
+def test_benchmark_networks_pass_the_pilot_rule(S, R, seed, t_end, samples, extra):
+    """The benchmark's synthetic networks keep the generator's acceptance
+    rule: in a 64-simulation pilot no recorded count reaches 2^30 (far from
+    the int32 limit, so no run can end in OVERFLOW) and every simulation
+    finishes normally."""
+    from cutauleaping_b200 import inputs
+    from tests.netutil import oracle_run
+    net = inputs.synthetic(S, R, 64, seed=seed, t_end=t_end, samples=samples, **extra)
+    out, info = oracle_run(net, seed=1)
+    assert int(out.max()) < 2 ** 30
+    assert (info["status"] == 0).all()
