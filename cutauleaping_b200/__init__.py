@@ -37,7 +37,7 @@ INFO_DTYPE = np.dtype([
 
 # Every symbol include/ctl.h declares (checked by the tests).
 EXPORTS = [
-    "ctl_status_str", "ctl_last_error", "ctl_model_load", "ctl_model_create", "ctl_model_free",
+    "ctl_status_str", "ctl_last_error", "ctl_last_error_detail", "ctl_model_load", "ctl_model_create", "ctl_model_free",
     "ctl_model_dims_get", "ctl_model_hor", "ctl_rows_load", "ctl_run_cfg_default", "ctl_run",
     "ctl_run_device", "ctl_run_device_noalloc", "ctl_launch_query", "ctl_autotune", "ctl_graph_create", "ctl_graph_launch", "ctl_graph_free",
     "ctl_write_dynamics", "ctl_print_dynamics", "ctl_write_samples_binary", "ctl_write_run_report", "ctl_target_load", "ctl_target_free",
@@ -76,6 +76,7 @@ class CtlError(RuntimeError):
         L = lib()
         msg = L.ctl_status_str(status).decode()
         detail = L.ctl_last_error().decode()
+        self.detail = int(L.ctl_last_error_detail())
         super().__init__(f"{where}: {msg}" + (f": {detail}" if detail else ""))
 
 
@@ -94,6 +95,7 @@ def lib():
         L.ctl_status_str.restype = C.c_char_p
         L.ctl_status_str.argtypes = [st]
         L.ctl_last_error.restype = C.c_char_p
+        L.ctl_last_error_detail.restype = C.c_int32
         L.ctl_model_load.argtypes = [C.c_char_p, C.POINTER(P)]
         L.ctl_model_create.argtypes = [C.c_int32, C.c_int32, P, P, P, C.c_int32, P, C.c_int32, P,
                                        C.POINTER(P)]

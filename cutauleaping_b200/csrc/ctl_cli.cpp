@@ -56,10 +56,15 @@ static void usage_exit() {
 static int exit_code(ctl_status st, const char* what) {
     std::string msg = ctl_last_error();
     fprintf(stderr, "ERROR (%s): %s%s%s\n", what, ctl_status_str(st), msg.empty() ? "" : ": ", msg.c_str());
-    // Map to the reference's exit codes (tau.cu:70,246,598,630,646,1139).
-    if (msg.find("do not fit") != std::string::npos) return -4;
-    if (msg.find("MX_0") != std::string::npos) return st == CTL_ERR_IO ? -6 : -5;
-    if (msg.find("cannot assign threads") != std::string::npos) return -10;
+    // The reference's exit codes (tau.cu:70,246,598,630,646,1139), from the
+    // status and its detail code, never from the message text.
+    switch (ctl_last_error_detail()) {
+        case CTL_DETAIL_ROWS_SHORT: return -4;
+        case CTL_DETAIL_MX0_ROW: return -5;
+        case CTL_DETAIL_MX0_UNREADABLE: return -6;
+        case CTL_DETAIL_TARGET_ASSIGN: return -10;
+        default: break;
+    }
     if (st == CTL_ERR_OOM) return -3;
     return -1;
 }

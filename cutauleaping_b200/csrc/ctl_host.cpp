@@ -27,11 +27,23 @@
 namespace ctl {
 
 static thread_local std::string g_last_error;
+static thread_local int32_t g_last_detail = CTL_DETAIL_NONE;
 
-void set_error(const std::string& msg) { g_last_error = msg; }
+void set_error(const std::string& msg) {
+    g_last_error = msg;
+    g_last_detail = CTL_DETAIL_NONE;
+}
 
 static ctl_status fail(ctl_status s, const std::string& msg) {
     set_error(msg);
+    return s;
+}
+
+// A failure with its ctl_error_detail (what the command line maps to the
+// reference's exit codes).
+static ctl_status fail_d(ctl_status s, ctl_error_detail d, const std::string& msg) {
+    set_error(msg);
+    g_last_detail = d;
     return s;
 }
 
@@ -215,6 +227,7 @@ extern "C" const char* ctl_status_str(ctl_status s) {
 }
 
 extern "C" const char* ctl_last_error(void) { return ctl::g_last_error.c_str(); }
+extern "C" int32_t ctl_last_error_detail(void) { return ctl::g_last_detail; }
 
 static ctl_status model_create_impl(int32_t S, int32_t R, const int32_t* left,
                                        const int32_t* right, const int32_t* feed, int32_t ns,
@@ -322,19 +335,24 @@ static ctl_status rows_load_impl(const char* folder, int32_t S, int32_t R, uint3
     std::string f(folder);
     std::vector<std::string> lines, tok;
     // read_quantities_offset (tau.cu:570-649): exit(-6) / -4 / -5 become statuses.
-    if (!read_lines(f + "/MX_0", lines)) return fail(CTL_ERR_IO, "ERROR reading quantities matrix: " + f + "/MX_0");
+    if (!read_lines(f + "/MX_0", lines))
+        return fail_d(CTL_ERR_IO, CTL_DETAIL_MX0_UNREADABLE, "ERROR reading quantities matrix: " + f + "/MX_0");
     if ((uint64_t)offset + n > lines.size())
-        return fail(CTL_ERR_SHAPE, "ERROR: input files rows (" + std::to_string(lines.size()) +
-                                       ") and requested threads (" + std::to_string(n) + ") do not fit");
+        return fail_d(CTL_ERR_SHAPE, CTL_DETAIL_ROWS_SHORT,
+                      "ERROR: input files rows (" + std::to_string(lines.size()) + ") and requested threads (" +
+                          std::to_string(n) + ") do not fit");
     for (uint32_t i = 0; i < n; i++) {
         split_tabs(lines[offset + i], tok);
         if ((int)tok.size() != S)
-            return fail(CTL_ERR_SHAPE, "MX_0 row " + std::to_string(offset + i) + ": " + std::to_string(tok.size()) +
-                                           " quantities, expected " + std::to_string(S));
+            return fail_d(CTL_ERR_SHAPE, CTL_DETAIL_MX0_ROW,
+                          "MX_0 row " + std::to_string(offset + i) + ": " + std::to_string(tok.size()) +
+                              " quantities, expected " + std::to_string(S));
         for (int s = 0; s < S; s++) {
             double v;
-            if (!parse_double(tok[s], v)) return fail(CTL_ERR_PARSE, "MX_0: bad entry '" + tok[s] + "'");
-            if (!(v >= 0.0) || v > 2147483647.0) return fail(CTL_ERR_SHAPE, "MX_0: quantity out of range '" + tok[s] + "'");
+            if (!parse_double(tok[s], v))
+                return fail_d(CTL_ERR_PARSE, CTL_DETAIL_MX0_ROW, "MX_0: bad entry '" + tok[s] + "'");
+            if (!(v >= 0.0) || v > 2147483647.0)
+                return fail_d(CTL_ERR_SHAPE, CTL_DETAIL_MX0_ROW, "MX_0: quantity out of range '" + tok[s] + "'");
             X0[(size_t)i * S + s] = (int32_t)(uint32_t)v;
         }
     }
@@ -569,8 +587,9 @@ static ctl_status target_load_impl(const char* folder, const ctl_model* m, uint3
     if (pp > 127) return fail(CTL_ERR_SHAPE, "at most 127 experiments");
     t->experiments = pp;
     if (last != N)
-        return fail(CTL_ERR_SHAPE, "ERROR! cannot assign threads (" + std::to_string(N) + ") to initial conditions (" +
-                                       std::to_string(last) + "), aborting");
+        return fail_d(CTL_ERR_SHAPE, CTL_DETAIL_TARGET_ASSIGN,
+                      "ERROR! cannot assign threads (" + std::to_string(N) + ") to initial conditions (" +
+                          std::to_string(last) + "), aborting");
     // ts_matrix: one row per sample, first column the instant, then
     // experiments x repetitions x target_quantities counts.
     if (!read_lines(f + "/ts_matrix", lines)) return fail(CTL_ERR_IO, "WARNING: cannot open ts file (fitness unavailable)");

@@ -628,9 +628,10 @@ static ctl_status check_cfg(const ctl_run_cfg* cfg) {
 
 struct DeviceGuard {
     int prev = -1;
+    cudaError_t err = cudaSuccess;  // result of making the device current
     explicit DeviceGuard(int d) {
         cudaGetDevice(&prev);
-        cudaSetDevice(d);
+        err = cudaSetDevice(d);
     }
     ~DeviceGuard() {
         if (prev >= 0) cudaSetDevice(prev);
@@ -1268,6 +1269,12 @@ extern "C" ctl_status ctl_run_device_noalloc(ctl_model* m, const ctl_run_cfg* cf
         return CTL_ERR_ARG;
     }
     DeviceGuard dg(cfg->device);
+    // The device must exist and be current before its copy of the array is
+    // looked up, and the launch must be possible before anything is written
+    // into the array: a call that fails leaves the shared array untouched.
+    if (dg.err != cudaSuccess) return cuda_fail(dg.err, "ctl_run_device_noalloc (cudaSetDevice)");
+    LaunchPlan pl;
+    if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;
     void* base = nullptr;
     {
         // Set-up, once per device with that device current: the host-side
@@ -1296,7 +1303,5 @@ extern "C" ctl_status ctl_run_device_noalloc(ctl_model* m, const ctl_run_cfg* cf
         return e == cudaSuccess;
     });
     if (e != cudaSuccess) return cuda_fail(e, "ctl_run_device_noalloc (tables)");
-    LaunchPlan pl;
-    if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;
     return enqueue_sweep(m, cfg, n, d_X0, d_c, d_samples, d_info, s, pl, d);
 }

@@ -7,7 +7,7 @@
  * (2phase_n-tau-leaping.cu:57-1261) and one output file per simulation
  * (2phase_n-tau-leaping.cu:3431-3507).  This header is the C ABI beneath
  * that boundary; the `cutauleaping` CLI is a thin wrapper over it, and any
- * host language binds it through its C FFI (see INTEGRATION.md).
+ * host language binds it through its C FFI.
  *
  * Conventions
  *   - Every entry point returns ctl_status; none calls exit().
@@ -41,6 +41,17 @@ typedef enum {
     CTL_ERR_TIMEOUT = 7,     /* reserved: bounded device waits gave up             */
     CTL_ERR_ARG = 8          /* invalid argument                                   */
 } ctl_status;
+
+/* Which input check failed, beside the status of the last failure
+ * (ctl_last_error_detail): the cases for which the reference's reader exits
+ * with its own code (2phase_n-tau-leaping.cu:598, 630, 646, 1139). */
+typedef enum {
+    CTL_DETAIL_NONE = 0,
+    CTL_DETAIL_MX0_UNREADABLE = 1, /* MX_0 missing or unreadable (reference: exit -6)        */
+    CTL_DETAIL_ROWS_SHORT = 2,     /* fewer MX_0 rows than offset + threads*blocks (-4)      */
+    CTL_DETAIL_MX0_ROW = 3,        /* an MX_0 row of the wrong length or a bad entry (-5)    */
+    CTL_DETAIL_TARGET_ASSIGN = 4   /* tts_vector does not cover threads*blocks (-10)         */
+} ctl_error_detail;
 
 /* Per-simulation status (ctl_sim_info.status). */
 typedef enum {
@@ -121,6 +132,9 @@ typedef struct {
 const char* ctl_status_str(ctl_status s);
 /* Message of the last failure on the calling thread ("" if none). */
 const char* ctl_last_error(void);
+/* ctl_error_detail of the last failure on the calling thread
+ * (CTL_DETAIL_NONE when the failure has no finer code). */
+int32_t ctl_last_error_detail(void);
 
 /* ---- models -------------------------------------------------------------- */
 /* Replaces first_pass + read_stoichiometry + read_instants

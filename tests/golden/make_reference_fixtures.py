@@ -50,11 +50,29 @@ def _syn12x20():
     return net
 
 
+def _syn32x64p():
+    """The uneven batch's synthetic segment: 32 species / 64 reactions
+    (generator seed 3), t_end 10, 200 samples, every simulation with its own
+    rate constants c * exp(0.5 z) (perturbation seed 31), 30 threads x 137
+    blocks = 4,110 simulations (the reference's shared memory holds 30
+    simulations of this network per block).  Reaction 0 is replaced by the
+    same positive zero-order inflow as in _syn12x20 (rate 1 in every row), so
+    the reference's critical-reaction search stays in bounds."""
+    net = inputs.synthetic(32, 64, 30 * 137, seed=3, t_end=10.0, samples=200, perturb_sigma=0.5,
+                           perturb_seed=31)
+    net.left[0] = 0
+    net.right[0] = 0
+    net.right[0, 0] = 1
+    net.c[:, 0] = 1.0
+    return net
+
+
 # name -> (network factory, threads, blocks, force_ssa, species columns kept raw)
 CASES = {
     "schlogl": (lambda: inputs.schlogl(4096), 64, 64, False, [1]),
     "schlogl_ssa": (lambda: inputs.schlogl(4096), 64, 64, True, [1]),
     "syn12x20": (_syn12x20, 32, 128, False, list(range(12))),
+    "syn32x64p": (_syn32x64p, 30, 137, False, list(range(0, 32, 4))),
 }
 RAW_EVERY = 10  # keep raw values at every 10th sample instant
 
@@ -91,7 +109,7 @@ def run_case(name, factory, threads, blocks, force, keep, outdir):
         args = [REF_BIN, folder, str(threads), str(blocks), "0", "0", os.path.join(td, "out"),
                 "pref", "0", "1" if force else "0", "2"]
         t0 = time.time()
-        p = subprocess.run(args, capture_output=True, text=True, timeout=900)
+        p = subprocess.run(args, capture_output=True, text=True, timeout=1200)
         wall = time.time() - t0
         if p.returncode != 0:
             raise RuntimeError(f"{name}: reference exited {p.returncode}: {p.stderr[-2000:]}")

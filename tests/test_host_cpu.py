@@ -99,15 +99,20 @@ def test_missing_optional_files(tmp_path):
     assert m.s_out == 3
 
 
-@pytest.mark.parametrize("edit,n,status", [
-    ({}, 9, ctl.ERR_SHAPE),                                        # read_quantities_offset exit(-4)
-    ({"MX_0": "1\t2\n" * 8}, 8, ctl.ERR_SHAPE),                    # exit(-5)
-    ({"MX_0": None}, 8, ctl.ERR_IO),                               # exit(-6)
-    ({"c_matrix": "1\t2\t3\n" * 8}, 8, ctl.ERR_SHAPE),             # too many / few parameters
-    ({"c_matrix": "1\t2\t3\t4\n" * 4}, 8, ctl.ERR_SHAPE),          # fewer rows than requested
-    ({"MX_0": "1\t-2\t3\n" * 8}, 8, ctl.ERR_SHAPE),                # negative population
+# ctl_error_detail codes (include/ctl.h): the CLI maps them to the
+# reference's exit codes -4, -5, -6 and -10.
+DETAIL_NONE, DETAIL_MX0_UNREADABLE, DETAIL_ROWS_SHORT, DETAIL_MX0_ROW, DETAIL_TARGET_ASSIGN = range(5)
+
+
+@pytest.mark.parametrize("edit,n,status,detail", [
+    ({}, 9, ctl.ERR_SHAPE, DETAIL_ROWS_SHORT),                               # read_quantities_offset exit(-4)
+    ({"MX_0": "1\t2\n" * 8}, 8, ctl.ERR_SHAPE, DETAIL_MX0_ROW),              # exit(-5)
+    ({"MX_0": None}, 8, ctl.ERR_IO, DETAIL_MX0_UNREADABLE),                  # exit(-6)
+    ({"c_matrix": "1\t2\t3\n" * 8}, 8, ctl.ERR_SHAPE, DETAIL_NONE),          # too many / few parameters
+    ({"c_matrix": "1\t2\t3\t4\n" * 4}, 8, ctl.ERR_SHAPE, DETAIL_NONE),       # fewer rows than requested
+    ({"MX_0": "1\t-2\t3\n" * 8}, 8, ctl.ERR_SHAPE, DETAIL_MX0_ROW),          # negative population
 ])
-def test_rows_load_errors(tmp_path, edit, n, status):
+def test_rows_load_errors(tmp_path, edit, n, status, detail):
     folder = _folder(tmp_path, **edit)
     m = ctl.Model.create(*[np.array(x) for x in ([[1, 2, 0], [0, 3, 0], [0, 0, 1], [0, 1, 0]],
                                                   [[0, 3, 0], [1, 2, 0], [0, 1, 0], [0, 0, 1]])],
@@ -115,6 +120,7 @@ def test_rows_load_errors(tmp_path, edit, n, status):
     with pytest.raises(ctl.CtlError) as e:
         ctl.load_rows(folder, m, 0, n)
     assert e.value.status == status
+    assert e.value.detail == detail
 
 
 def test_write_dynamics_format(tmp_path):
@@ -142,6 +148,9 @@ def test_fitness_target_load(tmp_path):
     assert (t.repetitions, t.p_rep, t.target_quantities, t.experiments) == (3, 2, 3, 2)
     with pytest.raises(ctl.CtlError):
         ctl.Target(folder, m, threads=2, blocks=3)   # p_rep does not divide blocks
+    with pytest.raises(ctl.CtlError) as e:
+        ctl.Target(folder, m, threads=2, blocks=6)   # tts_vector covers 8 of 12 simulations
+    assert e.value.detail == DETAIL_TARGET_ASSIGN
 
 
 def _cli(*args, cwd=None):

@@ -42,6 +42,22 @@ def _worker(rank, world, port, out_dir):
         dist.destroy_process_group()
 
 
+def test_merged_stats_keep_digits_at_large_counts():
+    """Counts near 1e6 over many simulations: the sum of squares passes 2^53,
+    so a variance from raw sums loses its digits; the pairwise merge of
+    per-part (count, mean, M2) keeps them."""
+    rng = np.random.default_rng(0)
+    x = (1_000_000 + rng.integers(-3, 4, size=(65536, 2, 3))).astype(np.float64)
+    exact_var = x.var(axis=0, ddof=1)
+    parts = [shard.local_stats(x[a:b]) for a, b in ((0, 1000), (1000, 40000), (40000, 65536))]
+    st = shard.merge_stats(parts)
+    assert np.array_equal(st[0], np.full((2, 3), 65536.0))
+    assert np.allclose(st[1], x.mean(0), rtol=1e-15, atol=0)
+    assert np.allclose(st[2] / 65535, exact_var, rtol=1e-9, atol=0)
+    raw = ((x * x).sum(0) - 65536 * x.mean(0) ** 2) / 65535
+    assert not np.allclose(raw, exact_var, rtol=1e-3, atol=0)   # what the merge avoids
+
+
 def test_shard_ranges_cover_the_batch():
     for n in (1, 7, 96, 1001):
         for world in (1, 2, 3, 8):

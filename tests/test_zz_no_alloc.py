@@ -46,6 +46,39 @@ def test_noalloc_matches_allocating_entry_on_two_calls():
         assert np.array_equal(got_info, ref_info), f"call {call}: records differ"
 
 
+@pytest.mark.gpu
+def test_noalloc_leaves_device_memory_unchanged():
+    """The promise itself: a call allocates no device memory.  After a
+    warm-up call of the same launch shape (which loads the kernel), a model
+    that the allocating entry has never seen runs through the no-alloc entry
+    with every buffer allocated beforehand, and the device's free memory is
+    the same before and after; its results then equal ctl_run_device's."""
+    import torch
+    L = ctl.lib()
+    net = inputs.synthetic(8, 12, 80, seed=21, t_end=0.8, samples=15, x0_range=(5, 500))
+    warm = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    _device_run(warm, net, L.ctl_run_device_noalloc, seed=5)
+    fresh = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).cuda()
+    c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).cuda()
+    out = torch.full((net.n, fresh.ns, fresh.s_out), -1, dtype=torch.int32, device="cuda")
+    info = torch.zeros((net.n, 40), dtype=torch.uint8, device="cuda")
+    cfg = ctl.run_cfg(seed=6)
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    st = L.ctl_run_device_noalloc(fresh.handle, C.byref(cfg), net.n, C.c_void_p(X0.data_ptr()),
+                                  C.c_void_p(c.data_ptr()), C.c_void_p(out.data_ptr()),
+                                  C.c_void_p(info.data_ptr()), C.c_void_p(stream.cuda_stream))
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert st == ctl.OK, L.ctl_last_error()
+    assert free_after == free_before, f"device memory changed by {free_before - free_after} bytes"
+    ref, ref_info = _device_run(fresh, net, L.ctl_run_device, seed=6)
+    assert np.array_equal(out.cpu().numpy(), ref)
+    assert np.array_equal(info.cpu().numpy(), ref_info)
+
+
 def test_noalloc_rejects_models_beyond_its_array():
     # 60000 reactions of two reactants: the packed tables alone exceed 1 MiB
     S, R = 200, 60000
