@@ -372,6 +372,9 @@ def main():
     ap.add_argument("--flags", type=int, default=0, help="run flags (quirk switches; 1 = forced SSA)")
     ap.add_argument("--ssa-budget", type=int, default=0, help="SSA steps per simulation and round (0 = library)")
     ap.add_argument("--dec-budget", type=int, default=0, help="leap decisions per simulation and round (0 = library)")
+    ap.add_argument("--warp-sims", type=int, default=0,
+                    help="tiny networks: simulations per warp of the register-resident sweep "
+                         "(0 = library choice, -1 = shared-memory sweep)")
     ap.add_argument("--autotune", action="store_true", help="measure launch shapes before timing")
     ap.add_argument("--no-autotune", action="store_true", help="config 3: library default shapes")
     ap.add_argument("--no-e2e", action="store_true")
@@ -430,7 +433,8 @@ def main():
         n = net.n
         cfg = ctl.run_cfg(seed=1 + si, sim_base=rank * n, device=local, group=a.group, threads=a.threads,
                           min_blocks=a.min_blocks, sched=a.sched, flags=a.flags, ssa_budget=a.ssa_budget,
-                          dec_budget=a.dec_budget, uniform_rates=int(bool((net.c == net.c[0]).all())))
+                          dec_budget=a.dec_budget, warp_sims=a.warp_sims,
+                          uniform_rates=int(bool((net.c == net.c[0]).all())))
         X0 = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).to(dev)
         c = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).to(dev)
         out = torch.empty((n, model.ns, model.s_out), dtype=torch.int32, device=dev)
@@ -580,6 +584,7 @@ def main():
                                    "smem_bytes": pt["li"].smem_bytes, "regs": pt["li"].regs_per_thread,
                                    "min_blocks": pt["li"].min_blocks, "sched": pt["li"].sched,
                                    "ssa_budget": pt["li"].ssa_budget, "dec_budget": pt["li"].dec_budget,
+                                   "warp_sims": pt["li"].warp_sims,
                                    "blocks_per_sm": pt["li"].blocks_per_sm} for pt in parts],
                        "autotuned": bool(a.autotune or (a.config == 3 and not a.no_autotune)),
                        "parallelism": f"dp{world} (independent simulations per rank)"},

@@ -25,7 +25,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-fmad=false", "-std=c++17",
                      "-Xcompiler", "-fPIC,-ffp-contract=off,-O3", f"-I{INCLUDE}"]
 
 GROUP_SIZES = (1, 2, 4, 8, 16, 32, 64, 128, 256)
-LIB_SOURCES = (["ctl_sweep.cu", "ctl_mlp.cu", "ctl_host.cpp"] +
+LIB_SOURCES = (["ctl_sweep.cu", "ctl_tiny.cu", "ctl_mlp.cu", "ctl_host.cpp"] +
                [f"ctl_sweep_g{g}.cu" for g in GROUP_SIZES])
 OBJ = os.path.join(HERE, "_obj")
 CLI_SOURCES = ["ctl_cli.cpp"]

@@ -66,7 +66,7 @@ struct ctl_model {
     std::mutex mu;
     ctl::DeviceCopy dev[16];
     // autotune cache: (device, log2 of the batch size, rate mode, flags) -> launch shape
-    struct Tuned { int device; uint32_t nbucket, uniform, flags; int group, threads, ssa_budget, dec_budget, min_blocks, sched; };
+    struct Tuned { int device; uint32_t nbucket, uniform, flags; int group, threads, ssa_budget, dec_budget, min_blocks, sched, warp_sims; };
     std::vector<Tuned> tuned;
 };
 

@@ -37,6 +37,7 @@
 #include "ctl_internal.h"
 
 #include "ctl_sweep_dev.cuh"
+#include "ctl_tiny.h"
 
 namespace ctl {
 namespace dev {
@@ -241,6 +242,8 @@ struct LaunchPlan {
     int ssa_budget = 0, dec_budget = 0;
     size_t smem = 0;
     dev::Layout lay{};
+    int warp_sims = 0;           // > 0: register-resident sweep, simulations per warp
+    int tinyP = 0, tinySM = 0;   // its kernel variant: tree leaves, species bound
 };
 
 // Stored levels of the sum tree for P = 2^k leaves: 3, 6, ... below k, then
@@ -449,6 +452,77 @@ static bool find_tuned(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, ctl_mod
 static int default_ssa_budget(bool one_wave) { return one_wave ? 8 : 16; }
 static int default_dec_budget(int G) { return G > 32 ? 2 : 1; }
 
+// Launch shape of the register-resident sweep for tiny networks: one thread
+// per simulation, `warp_sims` working lanes per warp.  Library choice of
+// warp_sims: spread a small batch so that about 8 warps per SM work (each
+// warp then runs the union of fewer simulations' paths), whole warps once the
+// batch fills them; smaller blocks while the batch would not reach every SM.
+struct TinyOcc {
+    int dev, P, SM, threads, bps, regs;
+};
+static std::vector<TinyOcc> g_tiny_occ;
+
+static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_t n, LaunchPlan& pl) {
+    DevAttr da;
+    if (device_attr(cfg->device, da) != CTL_OK) return CTL_ERR_CUDA;
+    pl.tinyP = t.P;
+    pl.tinySM = tiny_species_bound(t);
+    const void* k = tiny_kernel_ptr(pl.tinyP, pl.tinySM);
+    if (!k) {
+        set_error("no register-resident kernel for this network");
+        return CTL_ERR_SHAPE;
+    }
+    int ws = cfg->warp_sims;
+    if (ws <= 0) {
+        const uint64_t target_warps = (uint64_t)da.sm_count * 8;
+        ws = 1;
+        while (ws < 32 && (uint64_t)n > target_warps * (uint64_t)ws) ws <<= 1;
+    }
+    int threads = cfg->threads > 0 ? cfg->threads : 256;
+    if (threads % 32 || threads < 32 || threads > 256) {
+        set_error("threads per block must be a multiple of 32, at most 256");
+        return CTL_ERR_ARG;
+    }
+    const uint64_t warps = ((uint64_t)n + ws - 1) / ws;
+    if (cfg->threads <= 0)
+        while (threads > 32 && (warps * 32 + threads - 1) / threads < (uint64_t)da.sm_count) threads -= 32;
+    int bps = 0, regs = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_attr_mu);
+        for (const auto& o : g_tiny_occ)
+            if (o.dev == cfg->device && o.P == pl.tinyP && o.SM == pl.tinySM && o.threads == threads) {
+                bps = o.bps;
+                regs = o.regs;
+            }
+        if (!bps) {
+            cudaFuncAttributes fa;
+            CTL_CUDA(cudaFuncGetAttributes(&fa, k));
+            CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, 0));
+            regs = fa.numRegs;
+            g_tiny_occ.push_back({cfg->device, pl.tinyP, pl.tinySM, threads, bps, regs});
+        }
+    }
+    if (bps < 1) {
+        set_error("register-resident sweep cannot be resident with this shape");
+        return CTL_ERR_SHAPE;
+    }
+    const uint64_t need = (warps * 32 + threads - 1) / threads;
+    pl.G = 1;
+    pl.threads = threads;
+    pl.NS = threads / 32 * ws;
+    pl.blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)bps * da.sm_count));
+    pl.blocks_per_sm = bps;
+    pl.sm_count = da.sm_count;
+    pl.regs = regs;
+    pl.smem = 0;
+    pl.minb = 2;
+    pl.sched = 2;
+    pl.ssa_budget = cfg->ssa_budget > 0 ? cfg->ssa_budget : 16;
+    pl.dec_budget = 1;
+    pl.warp_sims = ws;
+    return CTL_OK;
+}
+
 static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t n, LaunchPlan& pl,
                               bool sums = false, bool use_tuned = true) {
     const HostTables& t = m->t;
@@ -462,9 +536,18 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
             if (tuned_cfg.dec_budget <= 0) tuned_cfg.dec_budget = e.dec_budget;
             if (tuned_cfg.min_blocks <= 0) tuned_cfg.min_blocks = e.min_blocks;
             if (tuned_cfg.sched <= 0) tuned_cfg.sched = e.sched;
+            if (tuned_cfg.warp_sims == 0) tuned_cfg.warp_sims = e.warp_sims;
         }
     }
     const ctl_run_cfg* cfg = &tuned_cfg;
+    const bool tiny_ok = tiny_eligible(t);
+    if (cfg->warp_sims > 0 && !tiny_ok) {
+        set_error("warp_sims: the register-resident sweep takes at most 16 reactions, 8 species, 8 sampled "
+                  "species and 3 reactant entries per reaction");
+        return CTL_ERR_ARG;
+    }
+    if (tiny_ok && (cfg->warp_sims > 0 || (cfg->warp_sims == 0 && cfg->group <= 0)))
+        return plan_tiny(t, cfg, n, pl);
     pl.ssa_budget = cfg->ssa_budget;
     pl.dec_budget = cfg->dec_budget;
     pl.sched = cfg->sched > 0 ? cfg->sched : 1;
@@ -578,6 +661,15 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.queue = d.ctrl;
     dev::Model dm = make_dev_model(m, d, cfg->flags);
     CTL_CUDA(cudaMemsetAsync(d.ctrl, 0, sizeof(uint32_t), stream));
+    if (pl.warp_sims > 0) {
+        tiny::Net net;
+        tiny_net(m->t, cfg->flags, dm.tvec, net);
+        uint32_t lanes = (uint32_t)pl.warp_sims;
+        void* targs[] = {&net, &run, &lanes};
+        CTL_CUDA(cudaLaunchKernel(tiny_kernel_ptr(pl.tinyP, pl.tinySM), dim3((unsigned)pl.blocks),
+                                  dim3((unsigned)pl.threads), targs, 0, stream));
+        return CTL_OK;
+    }
     void* args[] = {&dm, &run, const_cast<dev::Layout*>(&pl.lay)};
     CTL_CUDA(cudaLaunchKernel(kernel_for(pl.G, pl.minb), dim3((unsigned)pl.blocks), dim3((unsigned)pl.threads), args,
                               pl.smem, stream));
@@ -621,6 +713,10 @@ static ctl_status check_cfg(const ctl_run_cfg* cfg) {
     }
     if (cfg->sched < 0 || cfg->sched > 2) {
         set_error("sched must be 0 (library choice), 1 (block regrouping) or 2 (warp-local)");
+        return CTL_ERR_ARG;
+    }
+    if (cfg->warp_sims < -1 || cfg->warp_sims > 32) {
+        set_error("warp_sims must be -1 (never), 0 (library choice) or 1..32");
         return CTL_ERR_ARG;
     }
     return CTL_OK;
@@ -684,6 +780,7 @@ extern "C" ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uin
     li->sched = pl.sched;
     li->ssa_budget = pl.ssa_budget;
     li->dec_budget = pl.dec_budget;
+    li->warp_sims = pl.warp_sims;
     return CTL_OK;
 }
 
@@ -827,10 +924,12 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
 
 // Measured autotuner: times the library's own plan, then candidate launch
 // shapes greedily on the first `sample` simulations of the batch (results
-// are identical for every shape, only the time differs) -- group size,
-// threads per block, scheduling, register budget, then the per-round
-// budgets -- and caches the fastest for this (device, batch-size bucket,
-// rate mode, flags).  Nothing slower than the library's plan is cached.
+// are identical for every shape, only the time differs) -- for tiny networks
+// the register-resident sweep's simulations per warp; then lanes per
+// simulation, threads per block, scheduling and register budget of the
+// shared-memory sweep; then the per-round budgets -- and caches the fastest
+// for this (device, batch-size bucket, rate mode, flags).  Nothing slower
+// than the library's plan is cached.
 extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* d_X0,
                                    const float* d_c, uint32_t sample, ctl_launch_info* best) {
     if (!m || !d_X0 || !d_c || n == 0) return CTL_ERR_ARG;
@@ -849,6 +948,7 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
     c0.sched = 0;
     c0.ssa_budget = 0;
     c0.dec_budget = 0;
+    c0.warp_sims = 0;
     LaunchPlan p0;
     if ((st = plan_launch(m, &c0, n, p0, false, false)) != CTL_OK) return st;
     // A sample of about one wave of resident simulations is timed mostly by
@@ -865,14 +965,18 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
     cudaEventCreate(&e1);
     cudaError_t e = cudaMallocAsync(&dout, (size_t)k * t.ns * t.s_out * 4, s);
     if (e == cudaSuccess) e = cudaMallocAsync(&dinf, (size_t)k * sizeof(ctl_sim_info), s);
-    auto time_shape = [&](int G, int threads, int sb, int db, int mb, int sc, float& ms) -> ctl_status {
+    struct Shape {
+        int G, threads, ssa, dec, minb, sched, ws;  // ws > 0: register-resident sweep, else -1
+    };
+    auto time_shape = [&](const Shape& x, float& ms) -> ctl_status {
         ctl_run_cfg c = *cfg;
-        c.group = G;
-        c.threads = threads;
-        c.ssa_budget = sb;
-        c.dec_budget = db;
-        c.min_blocks = mb;
-        c.sched = sc;
+        c.group = x.ws > 0 ? 0 : x.G;
+        c.threads = x.threads;
+        c.ssa_budget = x.ssa;
+        c.dec_budget = x.dec;
+        c.min_blocks = x.ws > 0 ? 0 : x.minb;
+        c.sched = x.ws > 0 ? 0 : x.sched;
+        c.warp_sims = x.ws;
         LaunchPlan pl;
         ctl_status r = plan_launch(m, &c, k, pl, false, false);
         if (r != CTL_OK) return r;
@@ -885,60 +989,52 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         return CTL_OK;
     };
     const int S0 = p0.ssa_budget;
-    int bestG = p0.G, bestT = p0.threads, bestS = p0.ssa_budget, bestD = p0.dec_budget, bestM = p0.minb,
-        bestC = p0.sched;
+    Shape bestx{p0.G, p0.threads, p0.ssa_budget, p0.dec_budget, p0.minb, p0.sched,
+                p0.warp_sims > 0 ? p0.warp_sims : -1};
     float best_ms = 3.4e38f;
+    auto consider = [&](const Shape& x) {
+        float ms;
+        if (time_shape(x, ms) == CTL_OK && ms < best_ms) {
+            best_ms = ms;
+            bestx = x;
+        }
+    };
     if (e == cudaSuccess) {
-        {                                                  // 0. the library's own plan
-            float ms;
-            if (time_shape(bestG, bestT, bestS, bestD, bestM, bestC, ms) == CTL_OK) best_ms = ms;
+        consider(bestx);                                       // 0. the library's own plan
+        if (tiny_eligible(t))                                  // 1a. register-resident sweep
+            for (int ws : {1, 2, 4, 8, 16, 32})
+                if (ws != p0.warp_sims) consider({1, 0, S0 > 0 ? S0 : 16, 1, 2, 2, ws});
+        for (int G = 1; G <= 256 && G <= t.P; G <<= 1)        // 1b. lanes per simulation
+            if (G != p0.G || p0.warp_sims > 0) consider({G, 256, S0, default_dec_budget(G), 2, 1, -1});
+        const Shape b1 = bestx;
+        for (int th : {64, 128, 192, 256}) {                   // 2. threads per block
+            Shape x = b1;
+            x.threads = th;
+            if (th != b1.threads && (x.ws > 0 || (th % x.G == 0 && th >= x.G))) consider(x);
         }
-        for (int G = 1; G <= 256 && G <= t.P; G <<= 1) {  // 1. lanes per simulation
-            float ms;
-            if (G != p0.G && time_shape(G, 256, S0, default_dec_budget(G), 2, 1, ms) == CTL_OK && ms < best_ms) {
-                best_ms = ms;
-                bestG = G;
-                bestT = 256;
-                bestS = S0;
-                bestD = default_dec_budget(G);
-                bestM = 2;
-                bestC = 1;
+        if (bestx.ws <= 0) {
+            Shape x = bestx;                                   // 3. scheduling: warp-local vs block rounds
+            x.sched = bestx.sched == 2 ? 1 : 2;
+            consider(x);
+            const Shape b3 = bestx;
+            for (int mb : {2, 3, 4}) {                         // 4. register budget (resident blocks)
+                Shape y = b3;
+                y.minb = mb;
+                if (mb != b3.minb) consider(y);
             }
         }
-        for (int th : {64, 128, 192, 256}) {              // 2. threads per block
-            float ms;
-            if (th != bestT && th % bestG == 0 && th >= bestG &&
-                time_shape(bestG, th, bestS, bestD, bestM, bestC, ms) == CTL_OK && ms < best_ms) {
-                best_ms = ms;
-                bestT = th;
-            }
+        const Shape b4 = bestx;
+        for (int sb : {4, 8, 16, 32}) {                        // 5. SSA steps per round
+            Shape x = b4;
+            x.ssa = sb;
+            if (sb != b4.ssa) consider(x);
         }
-        {                                                  // 3. scheduling: warp-local vs block rounds
-            float ms;
-            const int sc = bestC == 2 ? 1 : 2;
-            if (time_shape(bestG, bestT, bestS, bestD, bestM, sc, ms) == CTL_OK && ms < best_ms) { best_ms = ms; bestC = sc; }
-        }
-        for (int mb : {2, 3, 4}) {                         // 4. register budget (resident blocks)
-            float ms;
-            if (mb != bestM && time_shape(bestG, bestT, bestS, bestD, mb, bestC, ms) == CTL_OK && ms < best_ms) {
-                best_ms = ms;
-                bestM = mb;
-            }
-        }
-        const int S1 = bestS;
-        for (int sb : {4, 8, 16, 32}) {                    // 5. SSA steps per round
-            float ms;
-            if (sb != S1 && time_shape(bestG, bestT, sb, bestD, bestM, bestC, ms) == CTL_OK && ms < best_ms) {
-                best_ms = ms;
-                bestS = sb;
-            }
-        }
-        const int D0 = bestD;
-        for (int db : {1, 2, 4}) {                         // 6. decisions per round
-            float ms;
-            if (db != D0 && time_shape(bestG, bestT, bestS, db, bestM, bestC, ms) == CTL_OK && ms < best_ms) {
-                best_ms = ms;
-                bestD = db;
+        if (bestx.ws <= 0) {
+            const Shape b5 = bestx;
+            for (int db : {1, 2, 4}) {                         // 6. decisions per round
+                Shape x = b5;
+                x.dec = db;
+                if (db != b5.dec) consider(x);
             }
         }
     }
@@ -953,14 +1049,16 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
     {
         std::lock_guard<std::mutex> lk(m->mu);
         const uint32_t nb = n_bucket(n), uni = (uint32_t)(cfg->uniform_rates != 0);
+        const ctl_model::Tuned tu{cfg->device, nb, uni, cfg->flags, bestx.ws > 0 ? 0 : bestx.G, bestx.threads,
+                                  bestx.ssa, bestx.dec, bestx.ws > 0 ? 0 : bestx.minb, bestx.ws > 0 ? 0 : bestx.sched,
+                                  bestx.ws};
         bool found = false;
         for (auto& x : m->tuned)
             if (x.device == cfg->device && x.nbucket == nb && x.uniform == uni && x.flags == cfg->flags) {
-                x.group = bestG; x.threads = bestT; x.ssa_budget = bestS; x.dec_budget = bestD; x.min_blocks = bestM;
-                x.sched = bestC;
+                x = tu;
                 found = true;
             }
-        if (!found) m->tuned.push_back({cfg->device, nb, uni, cfg->flags, bestG, bestT, bestS, bestD, bestM, bestC});
+        if (!found) m->tuned.push_back(tu);
     }
     if (best) {
         ctl_run_cfg c = *cfg;
@@ -968,6 +1066,7 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         c.threads = 0;
         c.min_blocks = 0;
         c.sched = 0;
+        c.warp_sims = 0;
         return ctl_launch_query(m, &c, n, best);
     }
     return CTL_OK;

@@ -1,0 +1,46 @@
+// Register-resident sweep for tiny networks: limits, the kernel's parameter
+// block and the host-side helpers (ctl_tiny.cu).  Not part of the C ABI.
+#pragma once
+
+#include <cstdint>
+
+#include "ctl_internal.h"
+
+namespace ctl {
+namespace tiny {
+
+constexpr int MAX_R = 16;  // reactions (tree leaves up to 16)
+constexpr int MAX_S = 8;   // species, and sampled species
+constexpr int MAX_E = 3;   // reactant entries per reaction
+
+// The model as a kernel parameter (constant bank; every value is the same
+// for all threads).  Species-major tables hold entries in ascending reaction
+// order, the reference's flattening order (tau.cu:314-342).
+struct Net {
+    int32_t S, R, ns, s_out;
+    double tmax;
+    const double* tvec;         // device copy of the sample instants
+    uint8_t ne[MAX_R];          // reactant entries of reaction r
+    uint8_t es[MAX_R][MAX_E];   // their species, ascending
+    uint8_t ec[MAX_R][MAX_E];   // their coefficients
+    int8_t V[MAX_S][MAX_R];     // tau1 table: V species-major (F when quirk Q5 is off)
+    uint8_t vnz[MAX_S];         // species s has an entry in V
+    int8_t Fm[MAX_S][MAX_R];    // feed-masked net change F, species-major (leap test)
+    uint8_t hor[MAX_S], hort[MAX_S];
+    uint8_t cs[MAX_S];          // sampled species
+    uint32_t frow[MAX_R][2];    // F reaction-major: 8 signed bytes per reaction (SSA update)
+};
+
+}  // namespace tiny
+
+// Networks the register-resident sweep runs: R <= 16, S <= 8, at most 8
+// sampled species, at most 3 reactant entries per reaction.
+bool tiny_eligible(const HostTables& t);
+// Species bound of the kernel variant (4 or 8).
+int tiny_species_bound(const HostTables& t);
+// Parameter block for a run with `flags` (quirk Q5 picks the tau1 table).
+void tiny_net(const HostTables& t, uint32_t flags, const double* d_tvec, tiny::Net& n);
+// Kernel for P tree leaves (2, 4, 8, 16) and species bound SM (4, 8).
+const void* tiny_kernel_ptr(int P, int SM);
+
+}  // namespace ctl

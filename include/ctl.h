@@ -111,6 +111,11 @@ typedef struct {
                              groups of 8+ lanes whose slots fit three blocks, else 2) */
     int32_t sched;        /* scheduling: 1 = block rounds regrouping simulations by phase,
                              2 = warp-local (no block barriers); 0 = library choice   */
+    int32_t warp_sims;    /* register-resident sweep for tiny networks (at most 16 reactions,
+                             8 species and sampled species, 3 reactant entries per reaction):
+                             simulations per warp, 1..32, one per thread; 0 = library
+                             choice (used for such networks unless `group` is set);
+                             -1 = never (shared-memory sweep)                         */
 } ctl_run_cfg;
 
 typedef struct {
@@ -126,6 +131,8 @@ typedef struct {
     int32_t min_blocks;   /* register budget of the kernel variant (ctl_run_cfg.min_blocks) */
     int32_t sched;        /* scheduling mode (ctl_run_cfg.sched) */
     int32_t ssa_budget, dec_budget;  /* work per simulation and round */
+    int32_t warp_sims;    /* simulations per warp of the register-resident sweep, 0 when the
+                             shared-memory sweep runs (ctl_run_cfg.warp_sims) */
 } ctl_launch_info;
 
 /* ---- errors ------------------------------------------------------------ */

@@ -84,6 +84,60 @@ def test_warp_local_scheduling_invariance(name, net):
     assert m.launch_info(net.n, sched=2).sched == 2
 
 
+TINY = [(n, net) for n, net in NETS if n in ("schlogl", "syn4x6", "syn8x12p", "feed3")]
+
+
+@pytest.mark.parametrize("name,net", TINY, ids=[n for n, _ in TINY])
+def test_register_resident_sweep_bit_exact(name, net):
+    """The register-resident sweep for tiny networks (one thread per
+    simulation, everything in registers) reproduces the oracle bit for bit
+    for any number of simulations per warp, block size and SSA budget; it
+    is the library's choice for these networks."""
+    out_o, info_o = oracle_run(net, seed=61)
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    assert m.launch_info(net.n).warp_sims > 0
+    assert m.launch_info(net.n, group=4).warp_sims == 0
+    for ws in (1, 3, 8, 32):
+        for threads in (32, 256):
+            for sb in (1, 16):
+                out, info = m.run(net.X0, net.c, seed=61, warp_sims=ws, threads=threads, ssa_budget=sb)
+                assert np.array_equal(out, out_o), f"{name} warp_sims={ws} threads={threads} ssa_budget={sb}"
+                assert same_info(info, info_o) is None, f"{name} warp_sims={ws} threads={threads}"
+                assert m.launch_info(net.n, warp_sims=ws, threads=threads).warp_sims == ws
+
+
+@pytest.mark.parametrize("flags", [ctl.FORCE_SSA, ctl.Q1_OFF, ctl.Q2_OFF, ctl.Q3_OFF, ctl.Q4_OFF,
+                                   ctl.Q5_OFF, ctl.Q6_OFF, ctl.Q9_OFF, ctl.Q10_OFF,
+                                   ctl.ALL_QUIRKS_OFF, ctl.ALL_QUIRKS_OFF | ctl.FORCE_SSA])
+def test_register_resident_quirk_switches(flags):
+    for name, net in TINY:
+        out_o, info_o = oracle_run(net, seed=8, flags=flags)
+        m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+        out, info = m.run(net.X0, net.c, seed=8, flags=flags, warp_sims=4)
+        assert np.array_equal(out, out_o), f"{name} flags={flags:#x}"
+        assert same_info(info, info_o) is None, f"{name} flags={flags:#x}"
+
+
+def test_register_resident_step_limit_and_sim_base():
+    name, net = TINY[0]
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    out, info = m.run(net.X0, net.c, seed=1, max_steps=50, check=False, warp_sims=2)
+    assert (info["status"] == ctl.SIM_STEP_LIMIT).all() and (info["steps"] == 50).all()
+    out_o, _ = oracle_run(net, seed=1, max_steps=50)
+    assert np.array_equal(out, out_o)
+    full, _ = m.run(net.X0, net.c, seed=5, warp_sims=8)
+    part, _ = m.run(net.X0[10:30], net.c[10:30], seed=5, sim_base=10, warp_sims=8)
+    assert np.array_equal(part, full[10:30])
+
+
+def test_register_resident_refuses_larger_networks():
+    name, net = [x for x in NETS if x[0] == "syn16x32"][0]
+    m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+    assert m.launch_info(net.n).warp_sims == 0
+    with pytest.raises(ctl.CtlError):
+        m.launch_info(net.n, warp_sims=4)
+
+
 def test_sim_base_selects_rows_of_a_larger_run():
     """The reference's `offset` shards rows; with sim_base the shard reproduces
     the same simulations a single large run produces."""
