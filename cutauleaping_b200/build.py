@@ -46,17 +46,36 @@ def _run(cmd, verbose):
     subprocess.run(cmd, check=True)
 
 
+# Headers that the library also hands to NVRTC at run time, to compile
+# kernels specialised for one network (ctl_tiny.cu): embedded as strings.
+EMBEDDED = (("ctl_src_devmath", "ctl_devmath.cuh"), ("ctl_src_tiny_body", "ctl_tiny_body.cuh"))
+
+
+def _embed_sources(path: str) -> None:
+    parts = ["// Generated by cutauleaping_b200/build.py: device sources for NVRTC.", "namespace ctl {"]
+    for sym, name in EMBEDDED:
+        text = open(os.path.join(CSRC, name)).read()
+        if ")CTLSRC\"" in text:
+            raise RuntimeError(f"{name} contains the raw-string delimiter")
+        parts.append(f'extern const char* const {sym} = R"CTLSRC({text})CTLSRC";')
+    parts.append("}  // namespace ctl")
+    open(path, "w").write("\n".join(parts) + "\n")
+
+
 def build(force: bool = False, verbose: bool = False) -> None:
     srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
     if force or _newer(LIB, srcs):
         # one object per translation unit, compiled in parallel, then linked
         os.makedirs(OBJ, exist_ok=True)
+        gen = os.path.join(OBJ, "ctl_tiny_src.cpp")
+        _embed_sources(gen)
+        srcs = srcs + [gen]
         objs = [os.path.join(OBJ, os.path.basename(s) + ".o") for s in srcs]
         cmds = [["nvcc", *NVCC_FLAGS, "-c", src, "-o", obj] for src, obj in zip(srcs, objs)]
         jobs = max(1, min(len(cmds), os.cpu_count() or 1))
         with ThreadPoolExecutor(jobs) as ex:
             list(ex.map(lambda c: _run(c, verbose), cmds))
-        _run(["nvcc", *ARCH, "-shared", "-o", LIB, *objs], verbose)
+        _run(["nvcc", *ARCH, "-shared", "-o", LIB, *objs, "-ldl"], verbose)
     cli_srcs = [os.path.join(CSRC, s) for s in CLI_SOURCES]
     if force or _newer(CLI, cli_srcs + [LIB]):
         _run(["g++", "-O2", "-std=c++17", f"-I{INCLUDE}", "-o", CLI, *cli_srcs,

@@ -244,6 +244,7 @@ struct LaunchPlan {
     dev::Layout lay{};
     int warp_sims = 0;           // > 0: register-resident sweep, simulations per warp
     int tinyP = 0, tinySM = 0;   // its kernel variant: tree leaves, species bound
+    const void* spec = nullptr;  // the kernel compiled for this network, if any
 };
 
 // Stored levels of the sum tree for P = 2^k leaves: 3, 6, ... below k, then
@@ -458,7 +459,9 @@ static int default_dec_budget(int G) { return G > 32 ? 2 : 1; }
 // warp then runs the union of fewer simulations' paths), whole warps once the
 // batch fills them; smaller blocks while the batch would not reach every SM.
 struct TinyOcc {
-    int dev, P, SM, threads, bps, regs;
+    int dev;
+    const void* kernel;
+    int threads, bps, regs;
 };
 static std::vector<TinyOcc> g_tiny_occ;
 
@@ -467,7 +470,8 @@ static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_
     if (device_attr(cfg->device, da) != CTL_OK) return CTL_ERR_CUDA;
     pl.tinyP = t.P;
     pl.tinySM = tiny_species_bound(t);
-    const void* k = tiny_kernel_ptr(pl.tinyP, pl.tinySM);
+    pl.spec = cfg->tiny_spec >= 0 ? tiny_spec_kernel(t, cfg->flags, nullptr) : nullptr;
+    const void* k = pl.spec ? pl.spec : tiny_kernel_ptr(pl.tinyP, pl.tinySM);
     if (!k) {
         set_error("no register-resident kernel for this network");
         return CTL_ERR_SHAPE;
@@ -490,7 +494,7 @@ static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_
     {
         std::lock_guard<std::mutex> lk(g_attr_mu);
         for (const auto& o : g_tiny_occ)
-            if (o.dev == cfg->device && o.P == pl.tinyP && o.SM == pl.tinySM && o.threads == threads) {
+            if (o.dev == cfg->device && o.kernel == k && o.threads == threads) {
                 bps = o.bps;
                 regs = o.regs;
             }
@@ -499,7 +503,7 @@ static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_
             CTL_CUDA(cudaFuncGetAttributes(&fa, k));
             CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, 0));
             regs = fa.numRegs;
-            g_tiny_occ.push_back({cfg->device, pl.tinyP, pl.tinySM, threads, bps, regs});
+            g_tiny_occ.push_back({cfg->device, k, threads, bps, regs});
         }
     }
     if (bps < 1) {
@@ -661,6 +665,13 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.queue = d.ctrl;
     dev::Model dm = make_dev_model(m, d, cfg->flags);
     CTL_CUDA(cudaMemsetAsync(d.ctrl, 0, sizeof(uint32_t), stream));
+    if (pl.warp_sims > 0 && pl.spec) {
+        SpecNet sn{dm.tvec, dm.tmax};
+        uint32_t lanes = (uint32_t)pl.warp_sims;
+        void* sargs[] = {&sn, &run, &lanes};
+        CTL_CUDA(cudaLaunchKernel(pl.spec, dim3((unsigned)pl.blocks), dim3((unsigned)pl.threads), sargs, 0, stream));
+        return CTL_OK;
+    }
     if (pl.warp_sims > 0) {
         tiny::Net net;
         tiny_net(m->t, cfg->flags, dm.tvec, net);
@@ -717,6 +728,10 @@ static ctl_status check_cfg(const ctl_run_cfg* cfg) {
     }
     if (cfg->warp_sims < -1 || cfg->warp_sims > 32) {
         set_error("warp_sims must be -1 (never), 0 (library choice) or 1..32");
+        return CTL_ERR_ARG;
+    }
+    if (cfg->tiny_spec < -1 || cfg->tiny_spec > 0) {
+        set_error("tiny_spec must be 0 (compile for the network when possible) or -1 (never)");
         return CTL_ERR_ARG;
     }
     return CTL_OK;
@@ -781,6 +796,7 @@ extern "C" ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uin
     li->ssa_budget = pl.ssa_budget;
     li->dec_budget = pl.dec_budget;
     li->warp_sims = pl.warp_sims;
+    li->specialized = pl.spec != nullptr ? 1 : 0;
     return CTL_OK;
 }
 
@@ -1372,6 +1388,11 @@ extern "C" ctl_status ctl_run_device_noalloc(ctl_model* m, const ctl_run_cfg* cf
     // looked up, and the launch must be possible before anything is written
     // into the array: a call that fails leaves the shared array untouched.
     if (dg.err != cudaSuccess) return cuda_fail(dg.err, "ctl_run_device_noalloc (cudaSetDevice)");
+    // Never a kernel compiled at run time here: loading one allocates device
+    // memory for its code.  The library's own kernels run instead.
+    ctl_run_cfg rc = *cfg;
+    rc.tiny_spec = -1;
+    cfg = &rc;
     LaunchPlan pl;
     if ((st = plan_launch(m, cfg, n, pl)) != CTL_OK) return st;
     void* base = nullptr;

@@ -3,15 +3,16 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 
 #include "ctl_internal.h"
 
 namespace ctl {
 namespace tiny {
 
-constexpr int MAX_R = 16;  // reactions (tree leaves up to 16)
-constexpr int MAX_S = 8;   // species, and sampled species
-constexpr int MAX_E = 3;   // reactant entries per reaction
+constexpr int MAX_R = 16;    // reactions (tree leaves up to 16)
+constexpr int MAX_S = 8;     // species, and sampled species
+constexpr int NET_MAX_E = 3; // reactant entries per reaction (the kernel body's MAX_E)
 
 // The model as a kernel parameter (constant bank; every value is the same
 // for all threads).  Species-major tables hold entries in ascending reaction
@@ -21,8 +22,8 @@ struct Net {
     double tmax;
     const double* tvec;         // device copy of the sample instants
     uint8_t ne[MAX_R];          // reactant entries of reaction r
-    uint8_t es[MAX_R][MAX_E];   // their species, ascending
-    uint8_t ec[MAX_R][MAX_E];   // their coefficients
+    uint8_t es[MAX_R][NET_MAX_E];  // their species, ascending
+    uint8_t ec[MAX_R][NET_MAX_E];  // their coefficients
     int8_t V[MAX_S][MAX_R];     // tau1 table: V species-major (F when quirk Q5 is off)
     uint8_t vnz[MAX_S];         // species s has an entry in V
     int8_t Fm[MAX_S][MAX_R];    // feed-masked net change F, species-major (leap test)
@@ -42,5 +43,16 @@ int tiny_species_bound(const HostTables& t);
 void tiny_net(const HostTables& t, uint32_t flags, const double* d_tvec, tiny::Net& n);
 // Kernel for P tree leaves (2, 4, 8, 16) and species bound SM (4, 8).
 const void* tiny_kernel_ptr(int P, int SM);
+
+// Parameter block of a model-specialised kernel: everything else is
+// compiled in.
+struct SpecNet {
+    const double* tvec;
+    double tmax;
+};
+// The kernel compiled for this network and tau1 table (quirk Q5 in flags)
+// by NVRTC, or nullptr when NVRTC is missing or the compilation failed (the
+// reason in *why).  Compiled once per process and network; takes a lock.
+const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, std::string* why);
 
 }  // namespace ctl

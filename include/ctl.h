@@ -116,6 +116,9 @@ typedef struct {
                              simulations per warp, 1..32, one per thread; 0 = library
                              choice (used for such networks unless `group` is set);
                              -1 = never (shared-memory sweep)                         */
+    int32_t tiny_spec;    /* register-resident sweep: 0 = run a kernel compiled at run time for
+                             this network (NVRTC; the library's own kernel when NVRTC is
+                             absent), -1 = the library's own kernel                    */
 } ctl_run_cfg;
 
 typedef struct {
@@ -133,6 +136,7 @@ typedef struct {
     int32_t ssa_budget, dec_budget;  /* work per simulation and round */
     int32_t warp_sims;    /* simulations per warp of the register-resident sweep, 0 when the
                              shared-memory sweep runs (ctl_run_cfg.warp_sims) */
+    int32_t specialized;  /* 1 when that sweep runs a kernel compiled for this network */
 } ctl_launch_info;
 
 /* ---- errors ------------------------------------------------------------ */

@@ -91,19 +91,25 @@ TINY = [(n, net) for n, net in NETS if n in ("schlogl", "syn4x6", "syn8x12p", "f
 def test_register_resident_sweep_bit_exact(name, net):
     """The register-resident sweep for tiny networks (one thread per
     simulation, everything in registers) reproduces the oracle bit for bit
-    for any number of simulations per warp, block size and SSA budget; it
-    is the library's choice for these networks."""
+    for any number of simulations per warp, block size and SSA budget, both
+    in the kernel compiled at run time for the network (NVRTC) and in the
+    library's own; the compiled one is the library's choice."""
     out_o, info_o = oracle_run(net, seed=61)
     m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
-    assert m.launch_info(net.n).warp_sims > 0
+    li = m.launch_info(net.n)
+    assert li.warp_sims > 0 and li.specialized == 1
+    assert m.launch_info(net.n, tiny_spec=-1).specialized == 0
     assert m.launch_info(net.n, group=4).warp_sims == 0
-    for ws in (1, 3, 8, 32):
-        for threads in (32, 256):
-            for sb in (1, 16):
-                out, info = m.run(net.X0, net.c, seed=61, warp_sims=ws, threads=threads, ssa_budget=sb)
-                assert np.array_equal(out, out_o), f"{name} warp_sims={ws} threads={threads} ssa_budget={sb}"
-                assert same_info(info, info_o) is None, f"{name} warp_sims={ws} threads={threads}"
-                assert m.launch_info(net.n, warp_sims=ws, threads=threads).warp_sims == ws
+    for spec in (0, -1):   # the kernel compiled for this network, the library's own
+        for ws in (1, 3, 8, 32):
+            for threads in (32, 256):
+                for sb in (1, 16):
+                    out, info = m.run(net.X0, net.c, seed=61, warp_sims=ws, threads=threads, ssa_budget=sb,
+                                      tiny_spec=spec)
+                    what = f"{name} spec={spec} warp_sims={ws} threads={threads} ssa_budget={sb}"
+                    assert np.array_equal(out, out_o), what
+                    assert same_info(info, info_o) is None, what
+                    assert m.launch_info(net.n, warp_sims=ws, threads=threads).warp_sims == ws
 
 
 @pytest.mark.parametrize("flags", [ctl.FORCE_SSA, ctl.Q1_OFF, ctl.Q2_OFF, ctl.Q3_OFF, ctl.Q4_OFF,
@@ -113,9 +119,10 @@ def test_register_resident_quirk_switches(flags):
     for name, net in TINY:
         out_o, info_o = oracle_run(net, seed=8, flags=flags)
         m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
-        out, info = m.run(net.X0, net.c, seed=8, flags=flags, warp_sims=4)
-        assert np.array_equal(out, out_o), f"{name} flags={flags:#x}"
-        assert same_info(info, info_o) is None, f"{name} flags={flags:#x}"
+        for spec in (0, -1):
+            out, info = m.run(net.X0, net.c, seed=8, flags=flags, warp_sims=4, tiny_spec=spec)
+            assert np.array_equal(out, out_o), f"{name} flags={flags:#x} spec={spec}"
+            assert same_info(info, info_o) is None, f"{name} flags={flags:#x} spec={spec}"
 
 
 def test_register_resident_step_limit_and_sim_base():
