@@ -233,11 +233,13 @@ static __device__ uint32_t poisson(double lam, uint32_t wa, uint32_t wb, uint64_
         return k;
     }
     double slam = sqrt(lam);
-    double loglam = dlog(lam);
     double b = 0.931 + 2.53 * slam;
     double a = -0.059 + 0.02483 * b;
-    double invalpha = 1.1239 + 1.1328 / (b - 3.4);
     double vr = 0.9277 - 3.6224 / (b - 2.0);
+    // log(lam) and log(1/alpha) only serve the slow acceptance test; most
+    // draws are accepted before it, so they are computed on its first use
+    double loglam = 0.0, log_invalpha = 0.0;
+    bool slow = false;
     uint4 w = make_uint4(0u, 0u, 0u, 0u);
     for (uint32_t t = 0; t < PTRS_MAX_TRIALS; t++) {
         if (t > 0) {
@@ -252,7 +254,12 @@ static __device__ uint32_t poisson(double lam, uint32_t wa, uint32_t wb, uint64_
         double k = floor((2.0 * a / us + b) * U + lam + 0.43);
         if (us >= 0.07 && V <= vr) return clamp_k(k);
         if (k < 0.0 || (us < 0.013 && V > us)) continue;
-        double lhs = dlog(V) + dlog(invalpha) - dlog(a / (us * us) + b);
+        if (!slow) {
+            loglam = dlog(lam);
+            log_invalpha = dlog(1.1239 + 1.1328 / (b - 3.4));
+            slow = true;
+        }
+        double lhs = dlog(V) + log_invalpha - dlog(a / (us * us) + b);
         double rhs = -lam + k * loglam - dlogfact(k);
         if (lhs <= rhs) return clamp_k(k);
     }

@@ -199,7 +199,7 @@ void accessor(std::ostringstream& o, const char* decl, int rows, int cols, F&& v
     o << " default: return 0; } }\n";
 }
 
-std::string spec_source(const HostTables& t, uint32_t flags) {
+std::string spec_source(const HostTables& t, uint32_t flags, int minb) {
     tiny::Net n;
     tiny_net(t, flags, nullptr, n);
     const int P = t.P, SM = tiny_species_bound(t);
@@ -223,7 +223,7 @@ std::string spec_source(const HostTables& t, uint32_t flags) {
     accessor(o, "unsigned cs(int a, int b = 0)", tiny::MAX_S, 1, [&](int i, int) { return (long long)n.cs[i]; });
     accessor(o, "unsigned frow(int a, int b)", tiny::MAX_R, 2, [&](int i, int j) { return (long long)n.frow[i][j]; });
     o << "};\n";
-    o << "extern \"C\" __global__ void __launch_bounds__(256, 2) ctl_tiny_spec("
+    o << "extern \"C\" __global__ void __launch_bounds__(256, " << minb << ") ctl_tiny_spec("
          "const __grid_constant__ NetCT net, const __grid_constant__ ctl::dev::Run run, unsigned lanes) {\n"
          "    ctl::tiny::sweep<NetCT, " << P << ", " << SM << ">(net, run, lanes);\n}\n";
     return o.str();
@@ -280,8 +280,8 @@ const void* compile_spec(const std::string& src, std::string& why) {
 
 }  // namespace
 
-const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, std::string* why) {
-    const std::string src = spec_source(t, flags & dev::F_Q5_OFF);
+const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, int minb, std::string* why) {
+    const std::string src = spec_source(t, flags & dev::F_Q5_OFF, minb);
     std::lock_guard<std::mutex> lk(g_spec_mu);
     for (const auto& e : g_spec)
         if (e.source == src) {

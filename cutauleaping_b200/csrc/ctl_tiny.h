@@ -51,8 +51,10 @@ struct SpecNet {
     double tmax;
 };
 // The kernel compiled for this network and tau1 table (quirk Q5 in flags)
-// by NVRTC, or nullptr when NVRTC is missing or the compilation failed (the
-// reason in *why).  Compiled once per process and network; takes a lock.
-const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, std::string* why);
+// by NVRTC, for minb resident 256-thread blocks per SM (its register
+// budget: 2, 3 or 4), or nullptr when NVRTC is missing or the compilation
+// failed (the reason in *why).  Compiled once per process, network and
+// budget; takes a lock.
+const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, int minb, std::string* why);
 
 }  // namespace ctl

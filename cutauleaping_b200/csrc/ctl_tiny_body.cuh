@@ -288,20 +288,22 @@ __device__ int decide_step(const N& net, const dev::Run& run, State<P, SM>& s, S
         build<P>(tc);
         a0c = tc[2 * P - 2];
     }
-    const uint4 wd = dev::draw(run.seed, 0u, dev::TAG_MISC, step, simg);
     double tau2 = (double)FLT_MAX;
-    if (a0c > 0.0) tau2 = -dev::dlog(dev::u53(wd.x, wd.y)) / a0c;
-    double tau = (double)tau1 < tau2 ? (double)tau1 : tau2;
     int pick_r = -1;
-    if ((double)tau1 > tau2) {
-        // the reference's linear search starts from PROP[0] unmasked (Q2):
-        // leaf 0 joins the tree when it is not critical itself
-        if (!(fl & dev::F_Q2_OFF) && !(crit & 1u)) {
-            tc[0] = (double)s.a[0];
-            build<P>(tc);
+    if (a0c > 0.0) {  // the draw serves tau2 and the critical pick only
+        const uint4 wd = dev::draw(run.seed, 0u, dev::TAG_MISC, step, simg);
+        tau2 = -dev::dlog(dev::u53(wd.x, wd.y)) / a0c;
+        if ((double)tau1 > tau2) {
+            // the reference's linear search starts from PROP[0] unmasked (Q2):
+            // leaf 0 joins the tree when it is not critical itself
+            if (!(fl & dev::F_Q2_OFF) && !(crit & 1u)) {
+                tc[0] = (double)s.a[0];
+                build<P>(tc);
+            }
+            pick_r = descend<P>(tc, dev::u53(wd.z, wd.w) * a0c);
         }
-        pick_r = descend<P>(tc, dev::u53(wd.z, wd.w) * a0c);
     }
+    double tau = (double)tau1 < tau2 ? (double)tau1 : tau2;
     uint32_t attempt = 0;
     uint32_t K[P];
     int32_t x1[SM];
@@ -450,8 +452,8 @@ __device__ __forceinline__ int ssa_step(const N& net, const dev::Run& run, State
 // One thread per simulation, `lanes` simulations per warp (lanes 0..lanes-1
 // of every warp work, the rest exit), simulations pulled from the device
 // work queue.  The working lanes of a warp take their SSA steps and their
-// leap decisions in lockstep phases (up to ssa_budget SSA steps, then one
-// decision) so that their instruction streams stay merged.
+// leap decisions in lockstep phases (up to ssa_budget SSA steps, then up to
+// dec_budget decisions) so that their instruction streams stay merged.
 template <class N, int P, int SM>
 __device__ __forceinline__ void sweep(const N& net, const dev::Run& run, uint32_t lanes) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -507,9 +509,10 @@ __device__ __forceinline__ void sweep(const N& net, const dev::Run& run, uint32_
             if (!__any_sync(mask, act)) break;
             if (act) res = ssa_step<N, P, SM>(net, run, s, st, o);
         }
-        {
+        for (uint32_t b = 0; b < run.dec_budget; b++) {
             const bool act = live && res == CONT && !st.in_ssa;
-            if (__any_sync(mask, act) && act) res = decide_step<N, P, SM>(net, run, s, st, o);
+            if (!__any_sync(mask, act)) break;
+            if (act) res = decide_step<N, P, SM>(net, run, s, st, o);
         }
         if (live && res == DONE) {
             if (o.samples)  // rows never reached read 0
