@@ -194,10 +194,29 @@ static uint32_t clamp_k(double k) {
  * Stream: primary block (0, TAG_POIS(attempt, r>>1), step, sim) gives the
  * pair (w0,w1) to even r and (w2,w3) to odd r; PTRS retries read extra
  * blocks 1 + 2j + (r&1), two trials per block.
- * lam < 10: sequential inversion from k = 0 (one uniform).
+ * lam < 10: sequential inversion from k = 0 (one uniform), p_k =
+ * p_{k-1} lam (1/k) with the correctly rounded reciprocals of recip_k.
  * lam >= 10: PTRS, W. Hormann, "The transformed rejection method for
  * generating Poisson random variables", Insurance: Mathematics and
  * Economics 12 (1993) 39-45. */
+static const double recip_k[64] = {
+    0x1.0000000000000p+0, 0x1.0000000000000p-1, 0x1.5555555555555p-2, 0x1.0000000000000p-2,
+    0x1.999999999999ap-3, 0x1.5555555555555p-3, 0x1.2492492492492p-3, 0x1.0000000000000p-3,
+    0x1.c71c71c71c71cp-4, 0x1.999999999999ap-4, 0x1.745d1745d1746p-4, 0x1.5555555555555p-4,
+    0x1.3b13b13b13b14p-4, 0x1.2492492492492p-4, 0x1.1111111111111p-4, 0x1.0000000000000p-4,
+    0x1.e1e1e1e1e1e1ep-5, 0x1.c71c71c71c71cp-5, 0x1.af286bca1af28p-5, 0x1.999999999999ap-5,
+    0x1.8618618618618p-5, 0x1.745d1745d1746p-5, 0x1.642c8590b2164p-5, 0x1.5555555555555p-5,
+    0x1.47ae147ae147bp-5, 0x1.3b13b13b13b14p-5, 0x1.2f684bda12f68p-5, 0x1.2492492492492p-5,
+    0x1.1a7b9611a7b96p-5, 0x1.1111111111111p-5, 0x1.0842108421084p-5, 0x1.0000000000000p-5,
+    0x1.f07c1f07c1f08p-6, 0x1.e1e1e1e1e1e1ep-6, 0x1.d41d41d41d41dp-6, 0x1.c71c71c71c71cp-6,
+    0x1.bacf914c1bad0p-6, 0x1.af286bca1af28p-6, 0x1.a41a41a41a41ap-6, 0x1.999999999999ap-6,
+    0x1.8f9c18f9c18fap-6, 0x1.8618618618618p-6, 0x1.7d05f417d05f4p-6, 0x1.745d1745d1746p-6,
+    0x1.6c16c16c16c17p-6, 0x1.642c8590b2164p-6, 0x1.5c9882b931057p-6, 0x1.5555555555555p-6,
+    0x1.4e5e0a72f0539p-6, 0x1.47ae147ae147bp-6, 0x1.4141414141414p-6, 0x1.3b13b13b13b14p-6,
+    0x1.3521cfb2b78c1p-6, 0x1.2f684bda12f68p-6, 0x1.29e4129e4129ep-6, 0x1.2492492492492p-6,
+    0x1.1f7047dc11f70p-6, 0x1.1a7b9611a7b96p-6, 0x1.15b1e5f75270dp-6, 0x1.1111111111111p-6,
+    0x1.0c9714fbcda3bp-6, 0x1.0842108421084p-6, 0x1.0410410410410p-6, 0x1.0000000000000p-6};
+
 uint32_t ctlo_poisson(double lam, uint64_t seed, uint32_t sim, uint32_t step,
                       uint32_t attempt, uint32_t r) {
     if (!(lam > 0.0)) return 0;
@@ -213,7 +232,7 @@ uint32_t ctlo_poisson(double lam, uint64_t seed, uint32_t sim, uint32_t step,
         uint32_t k = 0;
         while (u > F && k < 64) {
             k = k + 1;
-            p = (p * lam) / (double)k;
+            p = (p * lam) * recip_k[k - 1];
             F = F + p;
         }
         return k;
