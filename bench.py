@@ -447,6 +447,14 @@ def main():
         graph = model.graph(n, X0.data_ptr(), c.data_ptr(), out.data_ptr(), info.data_ptr(),
                             stream.cuda_stream, cfg)
         parts.append(dict(net=net, model=model, cfg=cfg, X0=X0, c=c, out=out, info=info, li=li, graph=graph))
+    # several segments (the uneven batch): one graph with a parallel branch per
+    # segment, so that one segment's tail overlaps the other's work
+    multi = None
+    if len(parts) > 1:
+        multi = ctl.graph_multi([(pt["model"], pt["net"].n, pt["X0"].data_ptr(), pt["c"].data_ptr(),
+                                  pt["out"].data_ptr(), pt["info"].data_ptr(), pt["cfg"]) for pt in parts],
+                                stream.cuda_stream)
+    launchers = [multi] if multi is not None else [pt["graph"] for pt in parts]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def barrier():
@@ -456,8 +464,8 @@ def main():
     with torch.cuda.stream(stream):
         for _ in range(a.warmup):
             flush.fill_(1)
-            for pt in parts:
-                pt["graph"].launch(stream.cuda_stream)
+            for g in launchers:
+                g.launch(stream.cuda_stream)
         stream.synchronize()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(a.steps)]
@@ -467,8 +475,8 @@ def main():
             for e0, e1 in ev:
                 flush.fill_(1)
                 e0.record(stream)
-                for pt in parts:
-                    pt["graph"].launch(stream.cuda_stream)
+                for g in launchers:
+                    g.launch(stream.cuda_stream)
                 e1.record(stream)
             stream.synchronize()
         torch.cuda.synchronize()
@@ -530,13 +538,22 @@ def main():
                 out=torch.empty((net.n, pt["model"].ns, pt["model"].s_out), dtype=torch.int32).pin_memory(),
                 info=torch.empty((net.n, 40), dtype=torch.uint8).pin_memory()))
 
+        def call_one(pt, h):
+            st = L.ctl_run(pt["model"].handle, C.byref(pt["cfg"]), pt["net"].n, C.c_void_p(h["X0"].data_ptr()),
+                           C.c_void_p(h["c"].data_ptr()), C.c_void_p(h["out"].data_ptr()),
+                           C.c_void_p(h["info"].data_ptr()))
+            if st not in (ctl.OK, ctl.ERR_STEP_LIMIT):
+                raise ctl.CtlError(st, "ctl_run")
+
         def call():
-            for pt, h in zip(parts, host):
-                st = L.ctl_run(pt["model"].handle, C.byref(pt["cfg"]), pt["net"].n, C.c_void_p(h["X0"].data_ptr()),
-                               C.c_void_p(h["c"].data_ptr()), C.c_void_p(h["out"].data_ptr()),
-                               C.c_void_p(h["info"].data_ptr()))
-                if st not in (ctl.OK, ctl.ERR_STEP_LIMIT):
-                    raise ctl.CtlError(st, "ctl_run")
+            # one host thread per segment: the calls (each on its own streams)
+            # run side by side, as the segments' branches do in the graph
+            if len(parts) == 1:
+                call_one(parts[0], host[0])
+                return
+            from concurrent.futures import ThreadPoolExecutor
+            with ThreadPoolExecutor(len(parts)) as ex:
+                list(ex.map(lambda ph: call_one(*ph), zip(parts, host)))
         call()
         barrier()
         et = []
@@ -587,6 +604,8 @@ def main():
                                    "warp_sims": pt["li"].warp_sims,
                                    "blocks_per_sm": pt["li"].blocks_per_sm} for pt in parts],
                        "autotuned": bool(a.autotune or (a.config == 3 and not a.no_autotune)),
+                       "graph": ("one CUDA graph per step, a parallel branch per segment" if multi is not None
+                                 else "one CUDA graph per step"),
                        "parallelism": f"dp{world} (independent simulations per rank)"},
             "roofline": {"bound": "hbm", "achieved": abytes / (ms * 1e-3) / 1e9,
                          "peak": hbm_peak, "unit": "GB/s",
@@ -611,6 +630,7 @@ def main():
         if io is not None:
             line["io"] = io
         print(json.dumps(line), flush=True)
+    del launchers, multi
     for pt in parts:
         del pt["graph"]
     if dist is not None:

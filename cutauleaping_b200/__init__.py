@@ -39,7 +39,7 @@ INFO_DTYPE = np.dtype([
 EXPORTS = [
     "ctl_status_str", "ctl_last_error", "ctl_last_error_detail", "ctl_model_load", "ctl_model_create", "ctl_model_free",
     "ctl_model_dims_get", "ctl_model_hor", "ctl_rows_load", "ctl_run_cfg_default", "ctl_run",
-    "ctl_run_device", "ctl_run_device_noalloc", "ctl_launch_query", "ctl_autotune", "ctl_graph_create", "ctl_graph_launch", "ctl_graph_free",
+    "ctl_run_device", "ctl_run_device_noalloc", "ctl_launch_query", "ctl_autotune", "ctl_graph_create", "ctl_graph_create_multi", "ctl_graph_launch", "ctl_graph_free",
     "ctl_write_dynamics", "ctl_print_dynamics", "ctl_write_samples_binary", "ctl_write_run_report", "ctl_target_load", "ctl_target_free",
     "ctl_target_dims", "ctl_fitness", "ctl_fitness_device", "ctl_mlp_gemm", "ctl_mlp_nll_grad", "ctl_mlp_colsum",
     "ctl_mlp_adam", "ctl_mlp_pack_bytes", "ctl_mlp_pack", "ctl_mlp_screen", "ctl_run_device_sums",
@@ -113,6 +113,7 @@ def lib():
         L.ctl_run_device_noalloc.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, P, P, P]
         L.ctl_autotune.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, C.c_uint32, C.POINTER(LaunchInfo)]
         L.ctl_graph_create.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, P, P, P, C.POINTER(P)]
+        L.ctl_graph_create_multi.argtypes = [C.c_uint32, P, P, P, P, P, P, P, P, C.POINTER(P)]
         L.ctl_graph_launch.argtypes = [P, P]
         L.ctl_graph_free.argtypes = [P]
         L.ctl_graph_free.restype = None
@@ -267,6 +268,21 @@ class Model:
         samples = np.ascontiguousarray(samples, dtype=np.uint32)
         _check(lib().ctl_write_samples_binary(self._h, os.fsencode(path), samples.shape[0], _p(samples),
                                               first_id), "ctl_write_samples_binary")
+
+
+def graph_multi(parts, stream=0) -> "Graph":
+    """One CUDA graph running several batches as parallel branches
+    (ctl_graph_create_multi).  parts: [(model, n, d_X0, d_c, d_out, d_info,
+    cfg)] with device pointers as ints; each model at most once."""
+    k = len(parts)
+    models = (C.c_void_p * k)(*[p[0].handle.value for p in parts])
+    cfgs = (RunCfg * k)(*[p[6] for p in parts])
+    ns = (C.c_uint32 * k)(*[p[1] for p in parts])
+    ptr = lambda i: (C.c_void_p * k)(*[p[i] for p in parts])
+    h = C.c_void_p()
+    _check(lib().ctl_graph_create_multi(k, models, cfgs, ns, ptr(2), ptr(3), ptr(4), ptr(5), C.c_void_p(stream),
+                                        C.byref(h)), "ctl_graph_create_multi")
+    return Graph(h.value)
 
 
 class Graph:

@@ -1129,6 +1129,88 @@ extern "C" ctl_status ctl_graph_create(ctl_model* m, const ctl_run_cfg* cfg, uin
     return CTL_OK;
 }
 
+// Several sweeps as parallel branches of one graph: a fork from the
+// capture stream into one stream per batch, joined back at the end.  The
+// persistent kernels then share the GPU: as one batch's blocks finish (its
+// queue drained), the next batch's blocks take their SMs, so a batch's
+// latency-bound tail overlaps the others' work (the reference runs such a
+// batch as separate processes or passes, kernel.cu:242-345).
+extern "C" ctl_status ctl_graph_create_multi(uint32_t count, ctl_model* const* models, const ctl_run_cfg* cfgs,
+                                             const uint32_t* n, const int32_t* const* d_X0,
+                                             const float* const* d_c, uint32_t* const* d_samples,
+                                             ctl_sim_info* const* d_info, void* stream, ctl_graph** out) {
+    if (!out) return CTL_ERR_ARG;
+    *out = nullptr;
+    if (count == 0 || count > 64 || !models || !cfgs || !n || !d_X0 || !d_c || !d_samples || !d_info) {
+        set_error("ctl_graph_create_multi: 1 to 64 batches with every array given");
+        return CTL_ERR_ARG;
+    }
+    const int device = cfgs[0].device;
+    for (uint32_t i = 0; i < count; i++) {
+        ctl_status st = check_cfg(&cfgs[i]);
+        if (st != CTL_OK) return st;
+        if (!models[i] || cfgs[i].device != device) {
+            set_error("ctl_graph_create_multi: every batch needs a model and the same device");
+            return CTL_ERR_ARG;
+        }
+        for (uint32_t j = 0; j < i; j++)
+            if (models[j] == models[i]) {  // one work-queue ticket per model and device
+                set_error("ctl_graph_create_multi: a model may appear once per graph");
+                return CTL_ERR_ARG;
+            }
+    }
+    DeviceGuard dg(device);
+    if (dg.err != cudaSuccess) return cuda_fail(dg.err, "ctl_graph_create_multi (cudaSetDevice)");
+    std::vector<DeviceCopy*> dcs(count, nullptr);
+    std::vector<LaunchPlan> pls(count);
+    for (uint32_t i = 0; i < count; i++) {
+        ctl_status st = ensure_device(models[i], device, dcs[i]);
+        if (st == CTL_OK) st = plan_launch(models[i], &cfgs[i], n[i], pls[i]);
+        if (st != CTL_OK) return st;
+    }
+    cudaStream_t cap = static_cast<cudaStream_t>(stream);
+    bool own = false;
+    if (cap == nullptr) {
+        CTL_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        own = true;
+    }
+    std::vector<cudaStream_t> br(count, nullptr);
+    std::vector<cudaEvent_t> ev(count + 1, nullptr);
+    cudaError_t e = cudaSuccess;
+    for (uint32_t i = 1; i < count && e == cudaSuccess; i++) e = cudaStreamCreateWithFlags(&br[i], cudaStreamNonBlocking);
+    for (uint32_t i = 0; i <= count && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+    ctl_graph* g = new ctl_graph();
+    g->device = device;
+    ctl_status st = CTL_OK;
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        cudaError_t ec = cudaEventRecord(ev[0], cap);  // fork
+        for (uint32_t i = 0; i < count && ec == cudaSuccess && st == CTL_OK; i++) {
+            cudaStream_t s = i == 0 ? cap : br[i];
+            if (i > 0) ec = cudaStreamWaitEvent(s, ev[0], 0);
+            if (ec == cudaSuccess)
+                st = enqueue_sweep(models[i], &cfgs[i], n[i], d_X0[i], d_c[i], d_samples[i], d_info[i], s, pls[i],
+                                   *dcs[i]);
+            if (i > 0 && ec == cudaSuccess && st == CTL_OK) ec = cudaEventRecord(ev[i], s);
+            if (i > 0 && ec == cudaSuccess && st == CTL_OK) ec = cudaStreamWaitEvent(cap, ev[i], 0);  // join
+        }
+        const cudaError_t e2 = cudaStreamEndCapture(cap, &g->graph);
+        e = ec != cudaSuccess ? ec : e2;
+    }
+    if (e == cudaSuccess && st == CTL_OK) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    for (auto s : br)
+        if (s) cudaStreamDestroy(s);
+    for (auto x : ev)
+        if (x) cudaEventDestroy(x);
+    if (own) cudaStreamDestroy(cap);
+    if (e != cudaSuccess || st != CTL_OK) {
+        ctl_graph_free(g);
+        return st != CTL_OK ? st : cuda_fail(e, "ctl_graph_create_multi");
+    }
+    *out = g;
+    return CTL_OK;
+}
+
 extern "C" ctl_status ctl_graph_launch(ctl_graph* g, void* stream) {
     if (!g || !g->exec) return CTL_ERR_ARG;
     DeviceGuard dg(g->device);

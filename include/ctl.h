@@ -214,6 +214,17 @@ ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const 
 ctl_status ctl_graph_create(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
                             const int32_t* d_X0, const float* d_c, uint32_t* d_samples,
                             ctl_sim_info* d_info, void* stream, ctl_graph** out);
+/* An uneven batch as one sweep: `count` batches (each its own model, run
+ * configuration, rows and output buffers on device) captured as parallel
+ * branches of ONE CUDA graph, so that the kernels share the GPU and one
+ * batch's latency-bound tail overlaps the others' work.  Replaces running the
+ * reference once per batch (its host loop, kernel.cu:242-345).  Every cfg
+ * names the same device; a model appears at most once (its work-queue
+ * ticket is per model and device). */
+ctl_status ctl_graph_create_multi(uint32_t count, ctl_model* const* models, const ctl_run_cfg* cfgs,
+                                  const uint32_t* n, const int32_t* const* d_X0, const float* const* d_c,
+                                  uint32_t* const* d_samples, ctl_sim_info* const* d_info, void* stream,
+                                  ctl_graph** out);
 ctl_status ctl_graph_launch(ctl_graph* g, void* stream);
 void ctl_graph_free(ctl_graph* g);
 

@@ -145,6 +145,43 @@ def test_register_resident_refuses_larger_networks():
         m.launch_info(net.n, warp_sims=4)
 
 
+def test_uneven_batch_as_one_graph_matches_separate_runs():
+    """Two batches of different networks (Schlogl on the register-resident
+    sweep, a perturbed 16 x 32 network on the shared-memory sweep) as the
+    parallel branches of one graph: each branch's results equal its own
+    separate run and the oracle, on two launches of the graph."""
+    import torch
+    stream = torch.cuda.current_stream().cuda_stream
+    nets = [NETS[0][1], [x for x in NETS if x[0] == "syn16x32"][0][1]]
+    parts, refs = [], []
+    for i, net in enumerate(nets):
+        m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+        X0 = torch.as_tensor(np.ascontiguousarray(net.X0, np.int32), device="cuda")
+        c = torch.as_tensor(np.ascontiguousarray(net.c, np.float32), device="cuda")
+        out = torch.full((net.n, m.ns, m.s_out), -1, dtype=torch.int32, device="cuda")
+        info = torch.zeros((net.n, 40), dtype=torch.uint8, device="cuda")
+        cfg = ctl.run_cfg(seed=13 + i, uniform_rates=int(bool((net.c == net.c[0]).all())))
+        parts.append((m, net.n, X0.data_ptr(), c.data_ptr(), out.data_ptr(), info.data_ptr(), cfg))
+        refs.append((m, X0, c, out, info))
+        ref_o, ref_i = m.run(net.X0, net.c, seed=13 + i)
+        orc_o, orc_i = oracle_run(net, seed=13 + i)
+        assert np.array_equal(ref_o, orc_o)
+        refs[-1] += (ref_o, ref_i)
+    g = ctl.graph_multi(parts, stream)
+    for _ in range(2):
+        for r in refs:
+            r[3].fill_(-1)
+            r[4].zero_()
+        g.launch(stream)
+        torch.cuda.synchronize()
+        for r in refs:
+            assert np.array_equal(r[3].cpu().numpy().view(np.uint32), r[5])
+            assert np.array_equal(r[4].cpu().numpy(), r[6].view(np.uint8).reshape(-1, 40))
+    with pytest.raises(ctl.CtlError):   # one model twice would share its queue ticket
+        ctl.graph_multi([parts[0], parts[0]], stream)
+    del g
+
+
 def test_sim_base_selects_rows_of_a_larger_run():
     """The reference's `offset` shards rows; with sim_base the shard reproduces
     the same simulations a single large run produces."""
