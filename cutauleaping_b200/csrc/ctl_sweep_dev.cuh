@@ -782,7 +782,7 @@ __device__ __forceinline__ Slot slot_of(unsigned char* smem, const Layout& lay, 
 template <int G, int MINB>
 __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layout lay) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ uint32_t s_cnt[3];  // SSA items, decision items, decision items done
+    __shared__ uint32_t s_cnt[2];
     const int NS = (int)(blockDim.x / G);
     const int gi = (int)(threadIdx.x / G);
     Grp<G> g;
@@ -880,7 +880,6 @@ __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layo
         if (threadIdx.x == 0) {
             s_cnt[0] = 0u;
             s_cnt[1] = 0u;
-            s_cnt[2] = 0u;
         }
         __syncthreads();
         for (int j = (int)threadIdx.x; j < NS; j += (int)blockDim.x) {
@@ -895,31 +894,21 @@ __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layo
         // The groups of a warp that work in the same phase step in lockstep:
         // before every step they agree (__any_sync over that phase's lanes)
         // whether anyone still has work, so their instruction streams merge.
-        // Decision items start at a warp boundary when they fit, so that no
-        // warp holds both phases; the SSA groups then keep stepping while any
-        // decision of the round is still running (a leap costs tens of SSA
-        // steps), instead of waiting for it at the round's barrier.
-        const uint32_t gpw = G < 32 ? 32u / G : 1u;
-        const uint32_t pad = (nssa + gpw - 1u) / gpw * gpw;
-        const uint32_t dbase = pad + ndec <= (uint32_t)NS ? pad : nssa;
         const uint32_t k = (uint32_t)gi;
+        const bool has_item = k < nssa + ndec;
         const bool is_ssa = k < nssa;
-        const bool is_dec = k >= dbase && k < dbase + ndec;
-        const bool has_item = is_ssa || is_dec;
         const uint32_t ssa_mask = __ballot_sync(0xffffffffu, is_ssa);
-        const uint32_t dec_mask = __ballot_sync(0xffffffffu, is_dec);
+        const uint32_t dec_mask = __ballot_sync(0xffffffffu, has_item && !is_ssa);
         if (has_item) {
-            const int j = (int)(is_ssa ? list[k] : list[NS - 1 - (int)(k - dbase)]);
+            const int j = (int)(is_ssa ? list[k] : list[NS - 1 - (int)(k - nssa)]);
             const Slot sl = slot_of<G>(smem, lay, j, NS, uni);
             Sim st;
             load_sim<G>(g, sa, j, st);
             const Out out = out_of(run, st.sim, sim_stride);
             int res = CONT;
             if (is_ssa) {
-                const uint32_t cap = 8u * run.ssa_budget;  // a round's longest SSA stretch
-                for (uint32_t b = 0; b < cap; b++) {
-                    const bool more = b < run.ssa_budget || *reinterpret_cast<volatile uint32_t*>(&s_cnt[2]) < ndec;
-                    const bool act = res == CONT && st.in_ssa && more;
+                for (uint32_t b = 0; b < run.ssa_budget; b++) {
+                    const bool act = res == CONT && st.in_ssa;
                     if (!__any_sync(ssa_mask, act)) break;
                     if (act) res = ssa_step<G>(g, m, run, sl, st, out);
                 }
@@ -929,8 +918,6 @@ __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layo
                     if (!__any_sync(dec_mask, act)) break;
                     if (act) res = decide_step<G>(g, m, run, sl, st, out);
                 }
-                g.sync();
-                if (g.lane == 0) atomicAdd(&s_cnt[2], 1u);
             }
             if (res == DONE) {
                 finish_sim<G>(g, m, run, st, out);
