@@ -461,9 +461,14 @@ static int default_dec_budget(int G) { return G > 32 ? 2 : 1; }
 struct TinyOcc {
     int dev;
     const void* kernel;
-    int threads, bps, regs;
+    int threads;
+    size_t smem;
+    int bps, regs;
 };
 static std::vector<TinyOcc> g_tiny_occ;
+
+// Scheduling of the register-resident sweep when the caller does not choose.
+static constexpr int TINY_DEFAULT_SCHED = 1;
 
 static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_t n, LaunchPlan& pl) {
     DevAttr da;
@@ -478,53 +483,72 @@ static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_
         set_error("no register-resident kernel for this network");
         return CTL_ERR_SHAPE;
     }
-    int ws = cfg->warp_sims;
-    if (ws <= 0) {
-        const uint64_t target_warps = (uint64_t)da.sm_count * 8;
-        ws = 1;
-        while (ws < 32 && (uint64_t)n > target_warps * (uint64_t)ws) ws <<= 1;
-    }
-    int threads = cfg->threads > 0 ? cfg->threads : 256;
-    if (threads % 32 || threads < 32 || threads > 256) {
-        set_error("threads per block must be a multiple of 32, at most 256");
+    const int sched = cfg->sched > 0 ? cfg->sched : TINY_DEFAULT_SCHED;
+    int threads = cfg->threads > 0 ? cfg->threads : (sched == 1 ? 64 : 256);
+    if (threads % 32 || threads < 32 || threads > 256 || (sched == 1 && threads < 64)) {
+        set_error("threads per block must be a multiple of 32, at most 256 (at least 64 for block rounds)");
         return CTL_ERR_ARG;
     }
-    const uint64_t warps = ((uint64_t)n + ws - 1) / ws;
-    // a batch of about one wave: blocks of two warps spread it evenly over the
-    // SMs (Schlogl, 4,096 simulations, 4 per warp: 230k against 212k sims/s
-    // with 192-thread blocks, which leave some SMs one block and others two)
-    if (cfg->threads <= 0 && warps <= (uint64_t)da.sm_count * 8) threads = 64;
+    int ws = cfg->warp_sims;
+    size_t smem = 0;
+    uint64_t need = 0;
+    if (sched == 1) {
+        // Block rounds with regrouping: `ws` live simulations per warp of the
+        // block on average, slots = ws * warps per block (at most 16 per warp
+        // leaves a whole warp for the deciding ones in a 64-thread block);
+        // a small batch is spread over every SM.
+        const uint64_t wpb = (uint64_t)threads / 32;
+        if (ws <= 0) {
+            const uint64_t per = ((uint64_t)n + (uint64_t)da.sm_count * wpb - 1) / ((uint64_t)da.sm_count * wpb);
+            ws = (int)std::min<uint64_t>(16, std::max<uint64_t>(1, per));
+        }
+        const uint64_t slots = (uint64_t)ws * wpb;
+        smem = (size_t)(2 * pl.tinySM + 18) * (size_t)threads * 4;
+        need = ((uint64_t)n + slots - 1) / slots;
+    } else {
+        if (ws <= 0) {
+            const uint64_t target_warps = (uint64_t)da.sm_count * 8;
+            ws = 1;
+            while (ws < 32 && (uint64_t)n > target_warps * (uint64_t)ws) ws <<= 1;
+        }
+        const uint64_t warps = ((uint64_t)n + ws - 1) / ws;
+        // a batch of about one wave: blocks of two warps spread it evenly over
+        // the SMs (Schlogl, 4,096 simulations, 4 per warp: 230k against 212k
+        // sims/s with 192-thread blocks, which leave some SMs one block and
+        // others two)
+        if (cfg->threads <= 0 && warps <= (uint64_t)da.sm_count * 8) threads = 64;
+        need = (warps * 32 + threads - 1) / threads;
+    }
     int bps = 0, regs = 0;
     {
         std::lock_guard<std::mutex> lk(g_attr_mu);
         for (const auto& o : g_tiny_occ)
-            if (o.dev == cfg->device && o.kernel == k && o.threads == threads) {
+            if (o.dev == cfg->device && o.kernel == k && o.threads == threads && o.smem == smem) {
                 bps = o.bps;
                 regs = o.regs;
             }
         if (!bps) {
             cudaFuncAttributes fa;
             CTL_CUDA(cudaFuncGetAttributes(&fa, k));
-            CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, 0));
+            CTL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads, smem));
             regs = fa.numRegs;
-            g_tiny_occ.push_back({cfg->device, k, threads, bps, regs});
+            g_tiny_occ.push_back({cfg->device, k, threads, smem, bps, regs});
         }
     }
     if (bps < 1) {
         set_error("register-resident sweep cannot be resident with this shape");
         return CTL_ERR_SHAPE;
     }
-    const uint64_t need = (warps * 32 + threads - 1) / threads;
     pl.G = 1;
     pl.threads = threads;
-    pl.NS = threads / 32 * ws;
+    pl.NS = sched == 1 ? ws * threads / 32 : threads / 32 * ws;
     pl.blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)bps * da.sm_count));
     pl.blocks_per_sm = bps;
     pl.sm_count = da.sm_count;
     pl.regs = regs;
-    pl.smem = 0;
+    pl.smem = smem;
     pl.minb = pl.spec ? minb : 2;
-    pl.sched = 2;
+    pl.sched = sched;
     pl.ssa_budget = cfg->ssa_budget > 0 ? cfg->ssa_budget : 16;
     pl.dec_budget = cfg->dec_budget > 0 ? cfg->dec_budget : 1;
     pl.warp_sims = ws;
@@ -669,20 +693,21 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.queue = d.ctrl;
     dev::Model dm = make_dev_model(m, d, cfg->flags);
     CTL_CUDA(cudaMemsetAsync(d.ctrl, 0, sizeof(uint32_t), stream));
-    if (pl.warp_sims > 0 && pl.spec) {
-        SpecNet sn{dm.tvec, dm.tmax};
-        uint32_t lanes = (uint32_t)pl.warp_sims;
-        void* sargs[] = {&sn, &run, &lanes};
-        CTL_CUDA(cudaLaunchKernel(pl.spec, dim3((unsigned)pl.blocks), dim3((unsigned)pl.threads), sargs, 0, stream));
-        return CTL_OK;
-    }
     if (pl.warp_sims > 0) {
-        tiny::Net net;
-        tiny_net(m->t, cfg->flags, dm.tvec, net);
-        uint32_t lanes = (uint32_t)pl.warp_sims;
-        void* targs[] = {&net, &run, &lanes};
-        CTL_CUDA(cudaLaunchKernel(tiny_kernel_ptr(pl.tinyP, pl.tinySM), dim3((unsigned)pl.blocks),
-                                  dim3((unsigned)pl.threads), targs, 0, stream));
+        // warp lockstep: simulations per warp; block rounds: live simulations per block
+        uint32_t lanes = (uint32_t)(pl.sched == 1 ? pl.NS : pl.warp_sims);
+        if (pl.spec) {
+            SpecNet sn{dm.tvec, dm.tmax};
+            void* sargs[] = {&sn, &run, &lanes};
+            CTL_CUDA(cudaLaunchKernel(pl.spec, dim3((unsigned)pl.blocks), dim3((unsigned)pl.threads), sargs, pl.smem,
+                                      stream));
+        } else {
+            tiny::Net net;
+            tiny_net(m->t, cfg->flags, dm.tvec, net);
+            void* targs[] = {&net, &run, &lanes};
+            CTL_CUDA(cudaLaunchKernel(tiny_kernel_ptr(pl.tinyP, pl.tinySM), dim3((unsigned)pl.blocks),
+                                      dim3((unsigned)pl.threads), targs, pl.smem, stream));
+        }
         return CTL_OK;
     }
     void* args[] = {&dm, &run, const_cast<dev::Layout*>(&pl.lay)};
@@ -995,7 +1020,7 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         c.ssa_budget = x.ssa;
         c.dec_budget = x.dec;
         c.min_blocks = x.ws > 0 ? 0 : x.minb;
-        c.sched = x.ws > 0 ? 0 : x.sched;
+        c.sched = x.sched;
         c.warp_sims = x.ws;
         LaunchPlan pl;
         ctl_status r = plan_launch(m, &c, k, pl, false, false);
@@ -1021,9 +1046,12 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
     };
     if (e == cudaSuccess) {
         consider(bestx);                                       // 0. the library's own plan
-        if (tiny_eligible(t))                                  // 1a. register-resident sweep
-            for (int ws : {1, 2, 4, 8, 16, 32})
-                if (ws != p0.warp_sims) consider({1, 0, S0 > 0 ? S0 : 16, 1, 2, 2, ws});
+        if (tiny_eligible(t)) {                                // 1a. register-resident sweep
+            for (int ws : {1, 2, 4, 8, 16, 32})                //     warp lockstep
+                if (!(ws == p0.warp_sims && p0.sched == 2)) consider({1, 0, S0 > 0 ? S0 : 16, 1, 2, 2, ws});
+            for (int ws : {4, 8, 12, 16})                      //     block rounds with regrouping
+                if (!(ws == p0.warp_sims && p0.sched == 1)) consider({1, 0, S0 > 0 ? S0 : 16, 1, 2, 1, ws});
+        }
         for (int G = 1; G <= 256 && G <= t.P; G <<= 1)        // 1b. lanes per simulation
             if (G != p0.G || p0.warp_sims > 0) consider({G, 256, S0, default_dec_budget(G), 2, 1, -1});
         const Shape b1 = bestx;
@@ -1070,8 +1098,7 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         std::lock_guard<std::mutex> lk(m->mu);
         const uint32_t nb = n_bucket(n), uni = (uint32_t)(cfg->uniform_rates != 0);
         const ctl_model::Tuned tu{cfg->device, nb, uni, cfg->flags, bestx.ws > 0 ? 0 : bestx.G, bestx.threads,
-                                  bestx.ssa, bestx.dec, bestx.ws > 0 ? 0 : bestx.minb, bestx.ws > 0 ? 0 : bestx.sched,
-                                  bestx.ws};
+                                  bestx.ssa, bestx.dec, bestx.ws > 0 ? 0 : bestx.minb, bestx.sched, bestx.ws};
         bool found = false;
         for (auto& x : m->tuned)
             if (x.device == cfg->device && x.nbucket == nb && x.uniform == uni && x.flags == cfg->flags) {

@@ -57,11 +57,11 @@ struct NetRT {
     __device__ __forceinline__ uint32_t frow(int r, int w) const { return n.frow[r][w]; }
 };
 
-// One thread per simulation, `lanes` simulations per warp; see sweep().
+// One thread per simulation; see run_sweep().
 template <int P, int SM>
 __global__ void __launch_bounds__(256, 2) tiny_kernel(const __grid_constant__ NetRT net,
                                                       const __grid_constant__ dev::Run run, uint32_t lanes) {
-    sweep<NetRT, P, SM>(net, run, lanes);
+    run_sweep<NetRT, P, SM>(net, run, lanes);
 }
 
 static_assert(NET_MAX_E == MAX_E, "parameter block and kernel body agree on reactant entries");
@@ -225,7 +225,7 @@ std::string spec_source(const HostTables& t, uint32_t flags, int minb) {
     o << "};\n";
     o << "extern \"C\" __global__ void __launch_bounds__(256, " << minb << ") ctl_tiny_spec("
          "const __grid_constant__ NetCT net, const __grid_constant__ ctl::dev::Run run, unsigned lanes) {\n"
-         "    ctl::tiny::sweep<NetCT, " << P << ", " << SM << ">(net, run, lanes);\n}\n";
+         "    ctl::tiny::run_sweep<NetCT, " << P << ", " << SM << ">(net, run, lanes);\n}\n";
     return o.str();
 }
 

@@ -454,13 +454,87 @@ __device__ __forceinline__ int ssa_step(const N& net, const dev::Run& run, State
 // work queue.  The working lanes of a warp take their SSA steps and their
 // leap decisions in lockstep phases (up to ssa_budget SSA steps, then up to
 // dec_budget decisions) so that their instruction streams stay merged.
+// Where simulation `sim` records its samples.
+__device__ __forceinline__ Out out_for(const dev::Run& run, uint32_t sim, size_t row_words) {
+    Out o;
+    if (run.sums) {
+        const uint32_t tp = run.sum_threads * run.sum_prep;
+        const uint32_t set = (sim / tp) * run.sum_threads + sim % run.sum_threads;
+        o.samples = nullptr;
+        o.sums = run.sums + (size_t)set * row_words;
+    } else {
+        o.samples = run.out + (size_t)sim * row_words;
+        o.sums = nullptr;
+    }
+    return o;
+}
+
+// The simulation's rate constants from its row of c (row 0 when every row is
+// the same), then its propensities and sum tree.
+template <class N, int P, int SM>
+__device__ __forceinline__ void load_rates(const N& net, const dev::Run& run, State<P, SM>& s, uint32_t sim) {
+#pragma unroll
+    for (int r = 0; r < P; r++)
+        s.c[r] = r < net.R() ? run.c[(run.uniform_c ? (size_t)0 : (size_t)sim * net.R()) + r] : 0.0f;
+    all_props<N, P, SM>(net, s);
+}
+
+// PrepareVariables (tau.cu:1269-1297).
+template <class N, int P, int SM>
+__device__ __forceinline__ void start_sim(const N& net, const dev::Run& run, State<P, SM>& s, Sim& st,
+                                          uint32_t sim) {
+#pragma unroll
+    for (int q = 0; q < SM; q++) {
+        s.x[q] = q < net.S() ? run.X0[(size_t)sim * net.S() + q] : 0;
+        s.last[q] = 0u;
+    }
+    load_rates<N, P, SM>(net, run, s, sim);
+    st.T = 0.0;
+    st.tl = 0.0;
+    st.t_next = net.tvec()[0];
+    st.fire = 0ull;
+    st.sim = sim;
+    st.cursor = st.n = st.burst = st.leaps = st.ssa = st.rej = 0u;
+    st.status = CTL_SIM_OK;
+    st.in_ssa = (run.flags & dev::F_FORCE_SSA) != 0;
+    st.pre = 0xffffffffu;
+}
+
+// The record of a finished simulation; rows never reached read 0.
+template <class N>
+__device__ __forceinline__ void finish(const N& net, const dev::Run& run, const Sim& st, const Out& o) {
+    const uint32_t ns = (uint32_t)net.ns();
+    if (o.samples)
+        for (uint32_t i = st.cursor; i < ns; i++)
+            for (int k = 0; k < net.s_out(); k++) o.samples[(size_t)i * net.s_out() + k] = 0u;
+    ctl_sim_info inf;
+    inf.t_final = st.T + st.tl;
+    inf.firings = st.fire;
+    inf.status = st.status;
+    inf.steps = st.n;
+    inf.leaps = st.leaps;
+    inf.ssa_steps = st.ssa;
+    inf.rejections = st.rej;
+    inf.pad = 0;
+    run.info[st.sim] = inf;
+    if (run.done) {  // publish: this simulation's rows and record are complete
+        __threadfence();
+        atomicAdd(run.done + (st.sim >> run.done_shift), 1u);
+    }
+}
+
+// Warp lockstep: one thread per simulation, `lanes` simulations per warp
+// (lanes 0..lanes-1 of every warp work, the rest exit), simulations pulled
+// from the device work queue.  The working lanes of a warp take their SSA
+// steps and their leap decisions in lockstep phases (up to ssa_budget SSA
+// steps, then up to dec_budget decisions) so that their instruction streams
+// stay merged; a lane in one phase waits while the others run the other.
 template <class N, int P, int SM>
 __device__ __forceinline__ void sweep(const N& net, const dev::Run& run, uint32_t lanes) {
     const uint32_t lane = threadIdx.x & 31u;
     if (lane >= lanes) return;
     const uint32_t mask = lanes >= 32 ? 0xffffffffu : ((1u << lanes) - 1u);
-    const uint32_t ns = (uint32_t)net.ns();
-    const size_t row_words = (size_t)ns * (size_t)net.s_out();
+    const size_t row_words = (size_t)net.ns() * (size_t)net.s_out();
     State<P, SM> s;
     Sim st;
     Out o{nullptr, nullptr};
@@ -471,34 +545,8 @@ __device__ __forceinline__ void sweep(const N& net, const dev::Run& run, uint32_
             if (sim >= run.n) {
                 closed = true;
             } else {
-                // PrepareVariables (tau.cu:1269-1297)
-#pragma unroll
-                for (int q = 0; q < SM; q++) {
-                    s.x[q] = q < net.S() ? run.X0[(size_t)sim * net.S() + q] : 0;
-                    s.last[q] = 0u;
-                }
-#pragma unroll
-                for (int r = 0; r < P; r++)
-                    s.c[r] = r < net.R() ? run.c[(run.uniform_c ? (size_t)0 : (size_t)sim * net.R()) + r] : 0.0f;
-                all_props<N, P, SM>(net, s);
-                st.T = 0.0;
-                st.tl = 0.0;
-                st.t_next = net.tvec()[0];
-                st.fire = 0ull;
-                st.sim = sim;
-                st.cursor = st.n = st.burst = st.leaps = st.ssa = st.rej = 0u;
-                st.status = CTL_SIM_OK;
-                st.in_ssa = (run.flags & dev::F_FORCE_SSA) != 0;
-                st.pre = 0xffffffffu;
-                if (run.sums) {
-                    const uint32_t tp = run.sum_threads * run.sum_prep;
-                    const uint32_t set = (sim / tp) * run.sum_threads + sim % run.sum_threads;
-                    o.samples = nullptr;
-                    o.sums = run.sums + (size_t)set * row_words;
-                } else {
-                    o.samples = run.out + (size_t)sim * row_words;
-                    o.sums = nullptr;
-                }
+                start_sim<N, P, SM>(net, run, s, st, sim);
+                o = out_for(run, sim, row_words);
                 live = true;
             }
         }
@@ -515,25 +563,184 @@ __device__ __forceinline__ void sweep(const N& net, const dev::Run& run, uint32_
             if (act) res = decide_step<N, P, SM>(net, run, s, st, o);
         }
         if (live && res == DONE) {
-            if (o.samples)  // rows never reached read 0
-                for (uint32_t i = st.cursor; i < ns; i++)
-                    for (int k = 0; k < net.s_out(); k++) o.samples[(size_t)i * net.s_out() + k] = 0u;
-            ctl_sim_info inf;
-            inf.t_final = st.T + st.tl;
-            inf.firings = st.fire;
-            inf.status = st.status;
-            inf.steps = st.n;
-            inf.leaps = st.leaps;
-            inf.ssa_steps = st.ssa;
-            inf.rejections = st.rej;
-            inf.pad = 0;
-            run.info[st.sim] = inf;
-            if (run.done) {  // publish: this simulation's rows and record are complete
-                __threadfence();
-                atomicAdd(run.done + (st.sim >> run.done_shift), 1u);
-            }
+            finish<N>(net, run, st, o);
             live = false;
         }
+    }
+}
+
+// Words of one simulation's resumable state in the regrouping exchange:
+// populations, the time and counters, the prepared random part of the next
+// SSA step and (fitness mode) the last recorded sample.  Rate constants,
+// propensities and the sum tree are rebuilt from them.
+template <int SM>
+struct Packed {
+    static constexpr int X = 0, T = SM, TL = SM + 2, FIRE = SM + 4, SIM = SM + 6, CURSOR = SM + 7, NSTEP = SM + 8,
+                         BURST = SM + 9, LEAPS = SM + 10, SSA = SM + 11, REJ = SM + 12, FLAGS = SM + 13,
+                         PRE = SM + 14, PREU = SM + 15, PRELG = SM + 17, LAST = SM + 18, WORDS = 2 * SM + 18;
+};
+
+// Word w of slot j: structure of arrays, consecutive slots in consecutive banks.
+template <int P, int SM>
+__device__ __forceinline__ void put_state(uint32_t* xs, uint32_t ns, uint32_t j, const State<P, SM>& s,
+                                          const Sim& st) {
+    using K = Packed<SM>;
+    auto w = [&](int i, uint32_t v) { xs[(uint32_t)i * ns + j] = v; };
+    auto w64 = [&](int i, unsigned long long v) {
+        w(i, (uint32_t)v);
+        w(i + 1, (uint32_t)(v >> 32));
+    };
+#pragma unroll
+    for (int q = 0; q < SM; q++) {
+        w(K::X + q, (uint32_t)s.x[q]);
+        w(K::LAST + q, s.last[q]);
+    }
+    w64(K::T, (unsigned long long)__double_as_longlong(st.T));
+    w64(K::TL, (unsigned long long)__double_as_longlong(st.tl));
+    w64(K::FIRE, st.fire);
+    w(K::SIM, st.sim);
+    w(K::CURSOR, st.cursor);
+    w(K::NSTEP, st.n);
+    w(K::BURST, st.burst);
+    w(K::LEAPS, st.leaps);
+    w(K::SSA, st.ssa);
+    w(K::REJ, st.rej);
+    w(K::FLAGS, (st.status << 1) | (st.in_ssa ? 1u : 0u));
+    w(K::PRE, st.pre);
+    w64(K::PREU, (unsigned long long)__double_as_longlong(st.pre_u));
+    w(K::PRELG, __float_as_uint(st.pre_lg));
+}
+
+template <class N, int P, int SM>
+__device__ __forceinline__ void get_state(const N& net, const uint32_t* xs, uint32_t ns, uint32_t j, State<P, SM>& s,
+                                          Sim& st) {
+    using K = Packed<SM>;
+    auto r = [&](int i) { return xs[(uint32_t)i * ns + j]; };
+    auto r64 = [&](int i) { return (unsigned long long)r(i) | ((unsigned long long)r(i + 1) << 32); };
+#pragma unroll
+    for (int q = 0; q < SM; q++) {
+        s.x[q] = (int32_t)r(K::X + q);
+        s.last[q] = r(K::LAST + q);
+    }
+    st.T = __longlong_as_double((long long)r64(K::T));
+    st.tl = __longlong_as_double((long long)r64(K::TL));
+    st.fire = r64(K::FIRE);
+    st.sim = r(K::SIM);
+    st.cursor = r(K::CURSOR);
+    st.n = r(K::NSTEP);
+    st.burst = r(K::BURST);
+    st.leaps = r(K::LEAPS);
+    st.ssa = r(K::SSA);
+    st.rej = r(K::REJ);
+    const uint32_t f = r(K::FLAGS);
+    st.status = f >> 1;
+    st.in_ssa = (f & 1u) != 0;
+    st.pre = r(K::PRE);
+    st.pre_u = __longlong_as_double((long long)r64(K::PREU));
+    st.pre_lg = __uint_as_float(r(K::PRELG));
+    st.t_next = st.cursor < (uint32_t)net.ns() ? net.tvec()[st.cursor] : 0.0;
+}
+
+// Block rounds with regrouping: at most `slots` simulations live in a block
+// (threads below `slots` take the first ones from the device work queue, and
+// a thread whose simulation ends takes the next one, so the count never
+// grows); every round the live simulations are sorted by phase -- SSA
+// first, then leap decisions from the next warp boundary -- and their state
+// moves through shared memory to the thread of their new position, so that
+// each warp runs one phase only (with slots <= 32 in a 64-thread block, warp
+// 0 steps SSA while warp 1 decides).  Then SSA threads take up to ssa_budget
+// steps and deciding threads up to dec_budget decisions, and the block meets
+// at a barrier.  xs: dynamic shared memory of Packed<SM>::WORDS words per
+// thread.
+template <class N, int P, int SM>
+__device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, uint32_t slots, uint32_t* xs) {
+    __shared__ uint32_t s_cnt[2][32];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t nt = blockDim.x, nw = nt >> 5;
+    const uint32_t below = (1u << lane) - 1u;
+    const size_t row_words = (size_t)net.ns() * (size_t)net.s_out();
+    State<P, SM> s;
+    Sim st;
+    Out o{nullptr, nullptr};
+    bool live = false;
+    if (tid < slots) {
+        const uint32_t sim = atomicAdd(run.queue, 1u);
+        if (sim < run.n) {
+            start_sim<N, P, SM>(net, run, s, st, sim);
+            live = true;
+        }
+    }
+    for (;;) {
+        const uint32_t bs = __ballot_sync(0xffffffffu, live && st.in_ssa);
+        const uint32_t bd = __ballot_sync(0xffffffffu, live && !st.in_ssa);
+        if (lane == 0) {
+            s_cnt[0][warp] = __popc(bs);
+            s_cnt[1][warp] = __popc(bd);
+        }
+        __syncthreads();
+        uint32_t nssa = 0, ndec = 0, offs = 0, offd = 0;
+        for (uint32_t w = 0; w < nw; w++) {
+            const uint32_t a = s_cnt[0][w], b = s_cnt[1][w];
+            if (w < warp) {
+                offs += a;
+                offd += b;
+            }
+            nssa += a;
+            ndec += b;
+        }
+        if (nssa + ndec == 0u) break;  // the same counts in every thread
+        const uint32_t pad = (nssa + 31u) & ~31u;
+        const uint32_t dbase = pad + ndec <= nt ? pad : nssa;
+        if (live) {
+            const uint32_t pos = st.in_ssa ? offs + __popc(bs & below) : dbase + offd + __popc(bd & below);
+            put_state<P, SM>(xs, nt, pos, s, st);
+        }
+        __syncthreads();
+        const bool mine_ssa = tid < nssa, mine_dec = tid >= dbase && tid < dbase + ndec;
+        live = mine_ssa || mine_dec;
+        if (live) {
+            get_state<N, P, SM>(net, xs, nt, tid, s, st);
+            load_rates<N, P, SM>(net, run, s, st.sim);
+            o = out_for(run, st.sim, row_words);
+        }
+        const uint32_t smask = __ballot_sync(0xffffffffu, mine_ssa);
+        const uint32_t dmask = __ballot_sync(0xffffffffu, mine_dec);
+        int res = CONT;
+        if (mine_ssa) {
+            for (uint32_t b = 0; b < run.ssa_budget; b++) {
+                const bool act = res == CONT && st.in_ssa;
+                if (!__any_sync(smask, act)) break;
+                if (act) res = ssa_step<N, P, SM>(net, run, s, st, o);
+            }
+        } else if (mine_dec) {
+            for (uint32_t b = 0; b < run.dec_budget; b++) {
+                const bool act = res == CONT && !st.in_ssa;
+                if (!__any_sync(dmask, act)) break;
+                if (act) res = decide_step<N, P, SM>(net, run, s, st, o);
+            }
+        }
+        if (live && res == DONE) {
+            finish<N>(net, run, st, o);
+            live = false;
+            const uint32_t sim = atomicAdd(run.queue, 1u);  // this thread's next simulation
+            if (sim < run.n) {
+                start_sim<N, P, SM>(net, run, s, st, sim);
+                live = true;
+            }
+        }
+    }
+}
+
+// The kernel body: warp lockstep (run.warp_local) or block rounds with
+// regrouping; `lanes` is the simulations per warp of the first and the live
+// simulations per block of the second.
+template <class N, int P, int SM>
+__device__ __forceinline__ void run_sweep(const N& net, const dev::Run& run, uint32_t lanes) {
+    if (run.warp_local) {
+        sweep<N, P, SM>(net, run, lanes);
+    } else {
+        extern __shared__ uint32_t ctl_tiny_xs[];
+        sweep_rounds<N, P, SM>(net, run, lanes, ctl_tiny_xs);
     }
 }
 

@@ -112,10 +112,12 @@ typedef struct {
     int32_t sched;        /* scheduling: 1 = block rounds regrouping simulations by phase,
                              2 = warp-local (no block barriers); 0 = library choice   */
     int32_t warp_sims;    /* register-resident sweep for tiny networks (at most 16 reactions,
-                             8 species and sampled species, 3 reactant entries per reaction):
-                             simulations per warp, 1..32, one per thread; 0 = library
-                             choice (used for such networks unless `group` is set);
-                             -1 = never (shared-memory sweep)                         */
+                             8 species and sampled species, 3 reactant entries per reaction),
+                             one thread per simulation: simulations per warp, 1..32 (with
+                             sched 1, block rounds that regroup the simulations by phase,
+                             the live simulations per warp of a block on average); 0 =
+                             library choice (used for such networks unless `group` is
+                             set); -1 = never (shared-memory sweep)                    */
     int32_t tiny_spec;    /* register-resident sweep: 0 = run a kernel compiled at run time for
                              this network (NVRTC; the library's own kernel when NVRTC is
                              absent), -1 = the library's own kernel                    */

@@ -75,8 +75,8 @@ def _both_paths(net, threads, p_rep, E, REP, seed, **cfgkw):
 
 
 @pytest.mark.parametrize("which", ["schlogl", "decay", "syn"])
-@pytest.mark.parametrize("sched,warp_sims", [(1, -1), (2, -1), (0, 4)],
-                         ids=["block-rounds", "warp-local", "register-resident"])
+@pytest.mark.parametrize("sched,warp_sims", [(1, -1), (2, -1), (2, 4), (1, 8)],
+                         ids=["block-rounds", "warp-local", "register-resident", "register-resident-rounds"])
 def test_sums_fitness_equals_sample_fitness(which, sched, warp_sims):
     if which == "schlogl":
         net, threads, p_rep = inputs.schlogl(96, samples=20, t_end=1.0), 8, 3

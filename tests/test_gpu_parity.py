@@ -100,16 +100,19 @@ def test_register_resident_sweep_bit_exact(name, net):
     assert li.warp_sims > 0 and li.specialized == 1
     assert m.launch_info(net.n, tiny_spec=-1).specialized == 0
     assert m.launch_info(net.n, group=4).warp_sims == 0
+    # sched 2: warp lockstep; sched 1: block rounds regrouping the simulations by phase
+    shapes = [(2, ws, th) for ws in (1, 3, 8, 32) for th in (32, 256)] + \
+             [(1, ws, th) for ws, th in ((1, 64), (3, 64), (16, 64), (5, 128), (32, 256))]
     for spec in (0, -1):   # the kernel compiled for this network, the library's own
-        for ws in (1, 3, 8, 32):
-            for threads in (32, 256):
-                for sb in (1, 16):
-                    out, info = m.run(net.X0, net.c, seed=61, warp_sims=ws, threads=threads, ssa_budget=sb,
-                                      tiny_spec=spec)
-                    what = f"{name} spec={spec} warp_sims={ws} threads={threads} ssa_budget={sb}"
-                    assert np.array_equal(out, out_o), what
-                    assert same_info(info, info_o) is None, what
-                    assert m.launch_info(net.n, warp_sims=ws, threads=threads).warp_sims == ws
+        for sched, ws, threads in shapes:
+            for sb, db in ((1, 1), (16, 2)):
+                out, info = m.run(net.X0, net.c, seed=61, warp_sims=ws, threads=threads, ssa_budget=sb,
+                                  dec_budget=db, sched=sched, tiny_spec=spec)
+                what = f"{name} spec={spec} sched={sched} warp_sims={ws} threads={threads} ssa_budget={sb}"
+                assert np.array_equal(out, out_o), what
+                assert same_info(info, info_o) is None, what
+                li = m.launch_info(net.n, warp_sims=ws, threads=threads, sched=sched)
+                assert li.warp_sims == ws and li.sched == sched
 
 
 @pytest.mark.parametrize("flags", [ctl.FORCE_SSA, ctl.Q1_OFF, ctl.Q2_OFF, ctl.Q3_OFF, ctl.Q4_OFF,
@@ -120,21 +123,23 @@ def test_register_resident_quirk_switches(flags):
         out_o, info_o = oracle_run(net, seed=8, flags=flags)
         m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
         for spec in (0, -1):
-            out, info = m.run(net.X0, net.c, seed=8, flags=flags, warp_sims=4, tiny_spec=spec)
-            assert np.array_equal(out, out_o), f"{name} flags={flags:#x} spec={spec}"
-            assert same_info(info, info_o) is None, f"{name} flags={flags:#x} spec={spec}"
+            for sched in (1, 2):
+                out, info = m.run(net.X0, net.c, seed=8, flags=flags, warp_sims=4, tiny_spec=spec, sched=sched)
+                assert np.array_equal(out, out_o), f"{name} flags={flags:#x} spec={spec} sched={sched}"
+                assert same_info(info, info_o) is None, f"{name} flags={flags:#x} spec={spec} sched={sched}"
 
 
 def test_register_resident_step_limit_and_sim_base():
     name, net = TINY[0]
     m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
-    out, info = m.run(net.X0, net.c, seed=1, max_steps=50, check=False, warp_sims=2)
-    assert (info["status"] == ctl.SIM_STEP_LIMIT).all() and (info["steps"] == 50).all()
     out_o, _ = oracle_run(net, seed=1, max_steps=50)
-    assert np.array_equal(out, out_o)
-    full, _ = m.run(net.X0, net.c, seed=5, warp_sims=8)
-    part, _ = m.run(net.X0[10:30], net.c[10:30], seed=5, sim_base=10, warp_sims=8)
-    assert np.array_equal(part, full[10:30])
+    for sched in (1, 2):
+        out, info = m.run(net.X0, net.c, seed=1, max_steps=50, check=False, warp_sims=2, sched=sched)
+        assert (info["status"] == ctl.SIM_STEP_LIMIT).all() and (info["steps"] == 50).all()
+        assert np.array_equal(out, out_o)
+        full, _ = m.run(net.X0, net.c, seed=5, warp_sims=8, sched=sched)
+        part, _ = m.run(net.X0[10:30], net.c[10:30], seed=5, sim_base=10, warp_sims=8, sched=sched)
+        assert np.array_equal(part, full[10:30])
 
 
 def test_register_resident_refuses_larger_networks():
