@@ -406,10 +406,6 @@ __device__ __forceinline__ int ssa_step(const N& net, const dev::Run& run, State
         ssa_randoms(run, simg, step, u, lg);
     }
     const int r = descend<P>(s.t, u * A0);
-    // the next step's random part, free of the state: it overlaps the
-    // update below (a leap decision in between leaves it unused)
-    ssa_randoms(run, simg, step + 1u, st.pre_u, st.pre_lg);
-    st.pre = step + 1u;
     const float dtf = -lg / (float)A0;
     st.tl = st.tl + (double)dtf;
     while (st.cursor < ns && st.T + st.tl > st.t_next) {
@@ -435,8 +431,14 @@ __device__ __forceinline__ int ssa_step(const N& net, const dev::Run& run, State
     }
     st.ssa++;
     st.fire += 1ull;
-    if (ovf) { st.status = CTL_SIM_OVERFLOW; return DONE; }
+    // Straight-line from the update to the new sum tree, with the next step's
+    // random part (free of the state; a leap decision in between leaves it
+    // unused) in the same block so that it fills the tree chain's stalls.
+    // After an overflow the propensities are computed and discarded.
+    ssa_randoms(run, simg, step + 1u, st.pre_u, st.pre_lg);
+    st.pre = step + 1u;
     all_props<N, P, SM>(net, s);
+    if (ovf) { st.status = CTL_SIM_OVERFLOW; return DONE; }
     st.burst++;
     if (st.cursor == ns) return DONE;
     if (st.burst == run.ssa_steps) {
