@@ -310,7 +310,8 @@ def bench_config5(a):
         reached = hist[-1][2] <= level
         return offset + hist[-1][0], hist[-1][1], reached, hist
     torch.cuda.synchronize()
-    tp, sp, plain_ok, ph = run_until("plain", 0.0)
+    plain_times, surr_times = [], []
+    tp, sp, plain_ok, ph = run_until("plain", 0.0, times=plain_times)
     t0 = time.perf_counter()
     theta, traj = fs.training_data(p, n_traj)
     torch.cuda.synchronize()
@@ -320,7 +321,12 @@ def bench_config5(a):
     t_train = time.perf_counter() - t0 - t_data
     ft_log = []
     ts, ss, surr_ok, sh = run_until("surrogate", t_data + t_train, screen=screen, keep_frac=0.01, net=net, sc=sc,
-                                    inner=a.inner, finetune_steps=a.finetune, replay=(theta, traj), log=ft_log)
+                                    inner=a.inner, finetune_steps=a.finetune, replay=(theta, traj), log=ft_log,
+                                    times=surr_times)
+    # the surrogate's own error where it matters: its predicted fitness at the
+    # true parameters and at the best candidate found, against simulation
+    pred = fs.predicted_fitness(p, net, sc, np.stack([p.theta_true, sh[-1][3]]))
+    sim_best = float(fs.true_fitness(p, sh[-1][3][None, :], seed=4243)[0])
     scr = screen_roofline(p, net, sc, n_cand=200_000)
     print(json.dumps({
         "metric": METRIC, "config": {"workload": "surrogate-screened parameter estimation: 32x64 network "
@@ -339,6 +345,11 @@ def bench_config5(a):
         "time_s": {"plain_to_level": tp, "surrogate_to_level": ts, "surrogate_data": t_data,
                    "surrogate_training": t_train},
         "generations": {"plain": len(ph), "surrogate": len(sh)},
+        "per_generation_s": {
+            "plain": [{k: round(v, 3) if isinstance(v, float) else v for k, v in x.items()} for x in plain_times],
+            "surrogate": [{k: round(v, 3) if isinstance(v, float) else v for k, v in x.items()} for x in surr_times]},
+        "surrogate_at": {"true_parameters": {"predicted": float(pred[0]), "simulated": truth},
+                         "best_found": {"predicted": float(pred[1]), "simulated_again": sim_best}},
         "finetune": {"phases": len(ft_log), "kept": sum(1 for x in ft_log if x["kept"]),
                      "surrogate_error": [[round(x["surrogate_error_before"], 4), round(x["after"], 4)]
                                          for x in ft_log]},

@@ -256,7 +256,8 @@ def _surrogate_error(p, net, sc, cand, f):
 
 def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_frac=0.01, net=None,
         sc=None, seed=0, sim_seed=1000, time_limit=None, stop_at=None, inner=1, explore_frac=0.0,
-        finetune_steps=0, finetune_reps=8, finetune_lr=2e-4, finetune_batch=8192, replay=None, log=None):
+        finetune_steps=0, finetune_reps=8, finetune_lr=2e-4, finetune_batch=8192, replay=None, log=None,
+        times=None):
     """Cross-entropy search in log-parameter space.
 
     mode 'plain' simulates every one of `pop` candidates per generation.
@@ -276,7 +277,9 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
     weights are kept only if the surrogate's error on that half went down.
     Every candidate whose fitness is reported was simulated.  Returns a list
     of (wall seconds, simulations so far, best true fitness, best theta), one
-    entry per generation; `log`, if a list, receives per-generation notes."""
+    entry per generation; `log`, if a list, receives per-generation notes, and
+    `times`, if a list, each generation's seconds of screening, re-simulation
+    (true fitness) and fine-tuning."""
     import torch
     rng = np.random.default_rng(seed)
     d = len(p.unknown)
@@ -288,6 +291,8 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
     sims = 0
     t0 = time.perf_counter()
     for gen in range(generations):
+        tg0 = time.perf_counter()
+        t_screen = t_ft = 0.0
         if mode == "plain":
             cand = np.clip(rng.normal(mu, sd, size=(pop, d)), p.log_lo, p.log_hi)
         else:
@@ -298,15 +303,18 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
                     el = big[order[: max(2, int(elite * keep_frac * screen))]]
                     mu = el.mean(0)
                     sd = np.maximum(el.std(0), floor)
+            t_screen = time.perf_counter() - tg0
             nk = max(pop, int(keep_frac * screen))
             nx = int(explore_frac * nk)
             cand = big[order[: nk - nx]]
             if nx:
                 cand = np.concatenate([cand, np.clip(rng.normal(mu, sd, size=(nx, d)), p.log_lo, p.log_hi)])
+        tr0 = time.perf_counter()
         if mode != "plain" and finetune_steps:
             f, traj = true_fitness(p, cand, seed=sim_seed + gen, sim_base=0, keep_reps=finetune_reps)
         else:
             f = true_fitness(p, cand, seed=sim_seed + gen, sim_base=0)
+        t_resim = time.perf_counter() - tr0
         sims += len(cand) * p.n_rep
         order = np.argsort(f)
         if f[order[0]] < best_f:
@@ -316,10 +324,14 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
         mu = el.mean(0)
         sd = np.maximum(el.std(0), floor)
         hist.append((time.perf_counter() - t0, sims, best_f, best_t))
+        if times is not None:
+            times.append({"gen": gen, "screen_s": t_screen, "resim_s": t_resim, "finetune_s": 0.0,
+                          "candidates": int(len(cand)), "best": best_f})
         if time_limit is not None and time.perf_counter() - t0 > time_limit:
             break
         if stop_at is not None and best_f <= stop_at:
             break
+        tf0 = time.perf_counter()
         if mode != "plain" and finetune_steps:
             reps = min(finetune_reps, p.n_rep)
             tr_idx, va_idx = np.arange(0, len(cand), 2), np.arange(1, len(cand), 2)
@@ -336,4 +348,6 @@ def cem(p: FitProblem, *, mode, generations, pop, elite=0.1, screen=None, keep_f
                 net.load_state(saved)
             if log is not None:
                 log.append({"gen": gen, "surrogate_error_before": before, "after": after, "kept": bool(kept)})
+        if times is not None:
+            times[-1]["finetune_s"] = time.perf_counter() - tf0
     return hist
