@@ -42,7 +42,7 @@ EXPORTS = [
     "ctl_run_device", "ctl_run_device_noalloc", "ctl_launch_query", "ctl_autotune", "ctl_graph_create", "ctl_graph_create_multi", "ctl_graph_launch", "ctl_graph_free",
     "ctl_write_dynamics", "ctl_print_dynamics", "ctl_write_samples_binary", "ctl_write_run_report", "ctl_target_load", "ctl_target_free",
     "ctl_target_dims", "ctl_fitness", "ctl_fitness_device", "ctl_mlp_gemm", "ctl_mlp_nll_grad", "ctl_mlp_colsum",
-    "ctl_mlp_adam", "ctl_mlp_pack_bytes", "ctl_mlp_pack", "ctl_mlp_screen", "ctl_run_device_sums",
+    "ctl_mlp_adam", "ctl_mlp_pack_bytes", "ctl_mlp_pack", "ctl_mlp_screen", "ctl_mlp_wait_check", "ctl_run_device_sums",
     "ctl_fitness_sums_device", "ctl_fitness_run",
 ]
 

@@ -70,9 +70,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait: returns false (and raises *err) after WAIT_LIMIT polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned* err) {
-    for (uint32_t i = 0; i < WAIT_LIMIT; i++) {
+// Bounded wait: returns false (and raises *err) after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned* err,
+                                          uint32_t limit = WAIT_LIMIT) {
+    for (uint32_t i = 0; i < limit; i++) {
         if (mbar_try_wait(bar, parity)) return true;
         if (i > 32) __nanosleep(64);
     }
@@ -748,6 +749,40 @@ static ctl_status mlp_cuda(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return CTL_OK;
     set_error(std::string(what) + ": " + cudaGetErrorString(e));
     return CTL_ERR_CUDA;
+}
+
+namespace ctl {
+namespace mlp {
+
+// One warp waits, through the same bounded wait as the GEMM and screening
+// kernels, on an mbarrier that nothing arrives on; no MMA or bulk copy is in
+// flight.  The wait gives up after `limit` polls, raises bit 0 of *err and
+// the kernel returns.
+__global__ void wait_check_kernel(unsigned* err, uint32_t limit) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (threadIdx.x == 0 && !mbar_wait(&bar, 0u, err, limit)) atomicOr(err, 2u);
+}
+
+}  // namespace mlp
+}  // namespace ctl
+
+extern "C" ctl_status ctl_mlp_wait_check(unsigned* d_err, uint32_t limit, void* stream) {
+    if (!d_err || limit == 0 || limit > mlp::WAIT_LIMIT) {
+        set_error("ctl_mlp_wait_check: a device error word and 1 <= limit <= 2^24");
+        return CTL_ERR_ARG;
+    }
+    mlp::wait_check_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(d_err, limit);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("ctl_mlp_wait_check: ") + cudaGetErrorString(e));
+        return CTL_ERR_CUDA;
+    }
+    return CTL_OK;
 }
 
 extern "C" ctl_status ctl_mlp_gemm(const ctl_gemm_desc* d, void* stream) {

@@ -375,6 +375,13 @@ size_t ctl_mlp_pack_bytes(int32_t out_w);
  * (row strides ldw[l] elements) for ctl_mlp_screen. */
 ctl_status ctl_mlp_pack(const void* const* W, const int32_t* ldw, int32_t out_w, void* wpack, void* stream);
 ctl_status ctl_mlp_screen(const ctl_screen_desc* d, void* stream);
+/* Checks the bounded waits of these kernels (no reference counterpart: the
+ * reference has no waits that can give up): one warp waits on an mbarrier
+ * that nothing arrives on, with nothing in flight, gives up after `limit`
+ * polls (1 .. 2^24) and returns; *d_err then has bits 0 (the wait raised
+ * its error) and 1 (the kernel saw the wait fail) set, which a caller reads
+ * as CTL_ERR_TIMEOUT. */
+ctl_status ctl_mlp_wait_check(unsigned* d_err, uint32_t limit, void* stream);
 
 #ifdef __cplusplus
 }

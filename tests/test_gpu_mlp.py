@@ -202,3 +202,28 @@ def test_screen_matches_layered_path():
     ref = _fitness_of_mean(mean, target)
     assert int(net.err.item()) == 0
     assert np.allclose(fit, ref, rtol=1e-5, atol=1e-9), np.abs(fit / ref - 1).max()
+
+
+def test_bounded_wait_gives_up_and_reports():
+    """The kernels' bounded mbarrier wait, on a barrier that nothing arrives
+    on (nothing in flight): it gives up after its poll limit, raises the
+    error word, the kernel returns (the context stays usable), and the
+    surrogate's host check turns the raised word into an error."""
+    import ctypes as C
+    import torch
+    L = ctl.lib()
+    L.ctl_mlp_wait_check.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = L.ctl_mlp_wait_check(C.c_void_p(err.data_ptr()), 4096, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == ctl.OK
+    torch.cuda.synchronize()
+    assert int(err.item()) == 3
+    assert L.ctl_mlp_wait_check(C.c_void_p(err.data_ptr()), 0, None) == ctl.ERR_ARG
+    # the context is still usable and the host side reports a raised word
+    from cutauleaping_b200 import surrogate as sg
+    net = sg.MLP(4, seed=0)
+    net.err.fill_(1)
+    with pytest.raises(RuntimeError):
+        net.check_error_flag()
+    net.err.zero_()
+    net.check_error_flag()
