@@ -211,6 +211,7 @@ def test_bounded_wait_gives_up_and_reports():
     surrogate's host check turns the raised word into an error."""
     import ctypes as C
     import torch
+    import cutauleaping_b200 as ctl
     L = ctl.lib()
     L.ctl_mlp_wait_check.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
