@@ -276,6 +276,60 @@ def bench_screen(a):
                       "roofline": r, "gpu_launches": 10}), flush=True)
 
 
+def bench_gemm(a):
+    """The surrogate's training GEMM alone (ctl_mlp_gemm, tcgen05): the
+    hidden-layer forward product of a 16,384-row training batch (M = 16384,
+    N = K = 256, bias + SiLU epilogue writing FP32 and BF16) and its weight
+    gradient (M = N = 256, K = 16384, split-K 8, FP32 atomic epilogue); 2MNK
+    FLOPs per launch, CUDA events on the launching stream over 20 launches
+    after 5 warm-ups; peak = the measured burst BF16 GEMM rate."""
+    import torch
+    from cutauleaping_b200 import surrogate as sg
+    g = torch.Generator(device="cuda").manual_seed(3)
+    B, W = 16384, 256
+    X = torch.randn(B, W, device="cuda", generator=g).to(torch.bfloat16)
+    Wt = (torch.randn(W, W, device="cuda", generator=g) / 16).to(torch.bfloat16)
+    bias = torch.zeros(W, device="cuda")
+    z = torch.empty(B, W, device="cuda")
+    h = torch.empty(B, W, dtype=torch.bfloat16, device="cuda")
+    XT = X.t().contiguous()
+    dW = torch.zeros(W, W, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    peaks, src = measured_peaks()
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    shapes = {
+        "forward (M=16384, N=256, K=256, bias+SiLU)": (lambda: sg.gemm(X, Wt, epilogue=sg.EPI_BIAS_SILU, out_f32=z,
+                                                                      out_bf=h, bias=bias, err=err), B * W * W),
+        "weight gradient (M=256, N=256, K=16384, split-K 8)": (lambda: sg.gemm(XT, XT, epilogue=sg.EPI_ATOMIC_F32,
+                                                                              out_f32=dW, splits=8, err=err), W * W * B),
+    }
+    out = {}
+    for name, (fn, mnk) in shapes.items():
+        for _ in range(5):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(20):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 20
+        ach = 2.0 * mnk / (ms * 1e-3) / 1e12
+        out[name] = {"launch_ms": ms, "achieved": ach, "frac": ach / peak}
+    if int(err.item()) != 0:
+        raise RuntimeError("GEMM reported a bounded-wait timeout")
+    fwd = out["forward (M=16384, N=256, K=256, bias+SiLU)"]
+    print(json.dumps({"metric": "training GEMM TFLOP/s (tcgen05, surrogate training shapes)",
+                      "value": fwd["achieved"], "unit": "TFLOP/s", "higher_is_better": True, "n_gpus": 1,
+                      "dtype": "bf16 (fp32 accumulate)", "data": "synthetic",
+                      "config": {"workload": "surrogate training GEMMs, 16,384-row batch, width 256"},
+                      "roofline": {"bound": "tensor", "achieved": fwd["achieved"], "peak": peak, "unit": "TFLOP/s",
+                                   "frac": fwd["frac"], "traffic": None,
+                                   "peak_source": f"MEASURED_PEAKS.json bf16_tflops ({src}, burst)"},
+                      "shapes": out, "gpu_launches": 50}), flush=True)
+
+
 def bench_config5(a):
     """Surrogate-screened parameter estimation against plain-simulator search.
 
@@ -373,6 +427,7 @@ def main():
     ap.add_argument("--time-limit", type=float, default=None,
                     help="config 5: wall-second cap per search (a capped plain search makes the speed-up a lower bound)")
     ap.add_argument("--screen-only", action="store_true", help="config 5: time the fused screening kernel alone")
+    ap.add_argument("--gemm-only", action="store_true", help="config 5: time the surrogate's training GEMM alone")
     ap.add_argument("--finetune", type=int, default=100,
                     help="config 5: surrogate fine-tuning steps per generation on the re-simulated trajectories")
     ap.add_argument("--sims", type=int, default=None, help="simulations per GPU (default: config's)")
@@ -398,6 +453,10 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if a.config == 5 and a.gemm_only:
+        if rank == 0 and a.impl == "ours":
+            bench_gemm(a)
+        return
     if a.config == 5 and a.screen_only:
         if rank == 0 and a.impl == "ours":
             bench_screen(a)
