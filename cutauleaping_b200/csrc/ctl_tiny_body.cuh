@@ -657,6 +657,10 @@ __device__ __forceinline__ void get_state(const N& net, const uint32_t* xs, uint
 template <class N, int P, int SM>
 __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, uint32_t slots, uint32_t* xs) {
     __shared__ uint32_t s_cnt[2][32];
+    // Warps that finished their share of the round, per round parity:
+    // [p][0] stepping warps after ssa_budget steps, [p][1] deciding warps
+    // after their decisions.
+    __shared__ uint32_t s_fin[2][2];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t nt = blockDim.x, nw = nt >> 5;
     const uint32_t below = (1u << lane) - 1u;
@@ -672,7 +676,9 @@ __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, 
             live = true;
         }
     }
-    for (;;) {
+    if (tid < 4) s_fin[tid >> 1][tid & 1] = 0u;
+    for (uint32_t round = 0;; round++) {
+        const uint32_t par = round & 1u;
         const uint32_t bs = __ballot_sync(0xffffffffu, live && st.in_ssa);
         const uint32_t bd = __ballot_sync(0xffffffffu, live && !st.in_ssa);
         if (lane == 0) {
@@ -691,8 +697,19 @@ __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, 
             ndec += b;
         }
         if (nssa + ndec == 0u) break;  // the same counts in every thread
+        // the other parity's flags were last read in the round before this one
+        if (tid < 2) s_fin[par ^ 1u][tid] = 0u;
         const uint32_t pad = (nssa + 31u) & ~31u;
         const uint32_t dbase = pad + ndec <= nt ? pad : nssa;
+        // Elastic rounds (when no warp holds both phases): a warp that has
+        // done its share keeps going while the other phase's warps still
+        // work -- stepping warps take further SSA steps, and in deciding
+        // warps the simulations that handed off to SSA take SSA steps --
+        // instead of waiting at the round's barrier.
+        const bool elastic = dbase == pad;
+        const uint32_t nsw = (nssa + 31u) >> 5;
+        const uint32_t ndw = ndec ? ((dbase + ndec - 1u) >> 5) - (dbase >> 5) + 1u : 0u;
+        volatile uint32_t* fin = s_fin[par];
         if (live) {
             const uint32_t pos = st.in_ssa ? offs + __popc(bs & below) : dbase + offd + __popc(bd & below);
             put_state<P, SM>(xs, nt, pos, s, st);
@@ -708,17 +725,32 @@ __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, 
         const uint32_t smask = __ballot_sync(0xffffffffu, mine_ssa);
         const uint32_t dmask = __ballot_sync(0xffffffffu, mine_dec);
         int res = CONT;
+        const uint32_t cap = 8u * run.ssa_budget;  // a round's longest SSA stretch
+        const bool first = lane == (uint32_t)(__ffs(mine_ssa ? smask : dmask) - 1);
         if (mine_ssa) {
-            for (uint32_t b = 0; b < run.ssa_budget; b++) {
-                const bool act = res == CONT && st.in_ssa;
+            bool told = false;
+            for (uint32_t b = 0; b < cap; b++) {
+                if (b == run.ssa_budget && first && !told) {
+                    atomicAdd((uint32_t*)&fin[0], 1u);
+                    told = true;
+                }
+                const bool more = b < run.ssa_budget || (elastic && fin[1] < ndw);
+                const bool act = res == CONT && st.in_ssa && more;
                 if (!__any_sync(smask, act)) break;
                 if (act) res = ssa_step<N, P, SM>(net, run, s, st, o);
             }
+            if (first && !told) atomicAdd((uint32_t*)&fin[0], 1u);
         } else if (mine_dec) {
             for (uint32_t b = 0; b < run.dec_budget; b++) {
                 const bool act = res == CONT && !st.in_ssa;
                 if (!__any_sync(dmask, act)) break;
                 if (act) res = decide_step<N, P, SM>(net, run, s, st, o);
+            }
+            if (first) atomicAdd((uint32_t*)&fin[1], 1u);
+            for (uint32_t b = 0; b < cap && elastic; b++) {
+                const bool act = res == CONT && st.in_ssa && fin[0] < nsw;
+                if (!__any_sync(dmask, act)) break;
+                if (act) res = ssa_step<N, P, SM>(net, run, s, st, o);
             }
         }
         if (live && res == DONE) {
