@@ -72,6 +72,8 @@ struct Run {
     unsigned long long* sums;        // fitness mode: [sets][ns][s_out] sample sums, else null
     uint32_t sum_threads, sum_prep;  // simulation -> parameter set (the reference's layout)
     uint32_t* done;                  // optional: finished simulations per chunk of 2^done_shift
+    uint32_t* out_host;              // optional: the caller's pinned rows [n][ns][s_out] (device view);
+                                     // each finished row is copied there by the kernel
     uint32_t done_shift;
     const int32_t* __restrict__ X0;  // [n][S]
     const float* __restrict__ c;     // [n][R]

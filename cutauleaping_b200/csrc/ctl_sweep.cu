@@ -671,7 +671,8 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
                                 const float* dc, uint32_t* dout, ctl_sim_info* dinfo,
                                 cudaStream_t stream, const LaunchPlan& pl, const DeviceCopy& d,
                                 unsigned long long* sums = nullptr, uint32_t sum_threads = 1,
-                                uint32_t sum_prep = 1, uint32_t* done = nullptr, uint32_t done_shift = 0) {
+                                uint32_t sum_prep = 1, uint32_t* done = nullptr, uint32_t done_shift = 0,
+                                uint32_t* out_host = nullptr) {
     dev::Run run;
     run.seed = cfg->seed;
     run.eps = cfg->eps;
@@ -694,6 +695,7 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.sum_prep = sum_prep;
     run.done = done;
     run.done_shift = done_shift;
+    run.out_host = out_host;
     run.info = dinfo;
     run.queue = d.ctrl;
     dev::Model dm = make_dev_model(m, d, cfg->flags);
@@ -881,14 +883,26 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
     const size_t bx = (size_t)n * t.S * 4, bc = (size_t)n * t.R * 4;
     const size_t row = (size_t)t.ns * t.s_out * 4, bo = (size_t)n * row, bi = (size_t)n * sizeof(ctl_sim_info);
     keep_pool_memory(cfg->device);
-    // Copy/compute overlap: the batch is cut into up to 16 chunks of 2^shift
-    // simulations; the kernel counts finished simulations per chunk (after a
-    // device-scope fence) and each complete chunk's rows are copied back on a
-    // second stream while the sweep goes on.
+    // A pinned caller buffer that the device can address: the kernel copies
+    // each finished simulation's row into it, so the copy-back runs inside
+    // the sweep with no host thread in the loop.
+    uint32_t* out_host = nullptr;
+    {
+        cudaPointerAttributes pa;
+        if (cudaPointerGetAttributes(&pa, samples) == cudaSuccess) {
+            if (pa.type == cudaMemoryTypeHost && pa.devicePointer) out_host = static_cast<uint32_t*>(pa.devicePointer);
+        } else {
+            cudaGetLastError();  // not a pointer CUDA knows: the copies below
+        }
+    }
+    // Otherwise copy/compute overlap: the batch is cut into up to 16 chunks of
+    // 2^shift simulations; the kernel counts finished simulations per chunk
+    // (after a device-scope fence) and each complete chunk's rows are copied
+    // back on a second stream while the sweep goes on.
     uint32_t shift = 0;
     while (((uint64_t)n >> shift) > 16) shift++;
     const uint32_t nch = (uint32_t)(((uint64_t)n + (1ull << shift) - 1) >> shift);
-    const bool overlap = bo >= ((size_t)64 << 20) && nch > 1;
+    const bool overlap = !out_host && bo >= ((size_t)64 << 20) && nch > 1;
     cudaStream_t s, cs;
     CTL_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
@@ -918,7 +932,7 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
     if (e == cudaSuccess) {
         st = enqueue_sweep(m, cfg, n, static_cast<int32_t*>(dx), static_cast<float*>(dc),
                            static_cast<uint32_t*>(dout), static_cast<ctl_sim_info*>(dinf), s, pl, *d, nullptr, 1, 1,
-                           static_cast<uint32_t*>(ddone), shift);
+                           static_cast<uint32_t*>(ddone), shift, out_host);
         if (st != CTL_OK) e = cudaErrorLaunchFailure;
     }
     std::vector<char> copied(nch, 0);
@@ -942,7 +956,7 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
             if (e == cudaSuccess) std::this_thread::sleep_for(std::chrono::microseconds(200));
         }
     }
-    for (uint32_t j = 0; j < nch && e == cudaSuccess; j++) {  // chunks not yet copied, after the sweep
+    for (uint32_t j = 0; j < nch && e == cudaSuccess && !out_host; j++) {  // chunks not yet copied, after the sweep
         const uint64_t lo = (uint64_t)j << shift, hi = std::min<uint64_t>(n, lo + (1ull << shift));
         if (!copied[j])
             e = cudaMemcpyAsync(reinterpret_cast<unsigned char*>(samples) + lo * row,

@@ -696,6 +696,22 @@ __device__ void finish_sim(const Grp<G>& g, const Model& m, const Run& run, cons
         inf.pad = 0;
         run.info[st.sim] = inf;
     }
+    if (run.out_host && out.samples) {
+        // the group's lanes wrote the rows; after the barrier every lane sees
+        // them and the group copies the simulation's row to the caller's
+        // pinned buffer (16-byte stores when the row allows)
+        g.sync();
+        const size_t words = (size_t)m.ns * (size_t)so;
+        const uint32_t* src = out.samples;
+        uint32_t* dst = run.out_host + (size_t)st.sim * words;
+        if ((words & 3u) == 0u && ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u) == 0u) {
+            const uint4* s4 = reinterpret_cast<const uint4*>(src);
+            uint4* d4 = reinterpret_cast<uint4*>(dst);
+            for (size_t i = g.lane; i < words / 4; i += G) d4[i] = s4[i];
+        } else {
+            for (size_t i = g.lane; i < words; i += G) dst[i] = src[i];
+        }
+    }
     if (run.done) {  // publish: this simulation's rows and record are complete
         __threadfence();
         g.sync();

@@ -502,6 +502,11 @@ __device__ __forceinline__ void start_sim(const N& net, const dev::Run& run, Sta
     st.pre = 0xffffffffu;
 }
 
+template <class N>
+__device__ __forceinline__ size_t row_words_of(const N& net) {
+    return (size_t)net.ns() * (size_t)net.s_out();
+}
+
 // The record of a finished simulation; rows never reached read 0.
 template <class N>
 __device__ __forceinline__ void finish(const N& net, const dev::Run& run, const Sim& st, const Out& o) {
@@ -519,6 +524,17 @@ __device__ __forceinline__ void finish(const N& net, const dev::Run& run, const 
     inf.rejections = st.rej;
     inf.pad = 0;
     run.info[st.sim] = inf;
+    if (run.out_host && o.samples) {  // the row to the caller's pinned buffer
+        const size_t words = row_words_of(net);
+        const uint32_t* src = o.samples;
+        uint32_t* dst = run.out_host + (size_t)st.sim * words;
+        if ((words & 3u) == 0u && (((unsigned long long)src | (unsigned long long)dst) & 15ull) == 0ull) {
+            for (size_t i = 0; i < words / 4; i++)
+                reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+        } else {
+            for (size_t i = 0; i < words; i++) dst[i] = src[i];
+        }
+    }
     if (run.done) {  // publish: this simulation's rows and record are complete
         __threadfence();
         atomicAdd(run.done + (st.sim >> run.done_shift), 1u);

@@ -250,6 +250,33 @@ def test_host_run_with_overlapped_copies_matches_device_run():
     assert np.array_equal(out_h[2300:2304], out_o)
 
 
+def test_host_run_into_pinned_buffers_writes_rows_from_the_kernel():
+    """With pinned (device-addressable) host buffers, ctl_run's kernel copies
+    each finished row into the caller's buffer itself: the rows and records
+    equal a device-resident run's, on the shared-memory sweep (rows of a
+    multiple of four words, 16-byte stores) and on the register-resident one
+    (Schlogl, 25 instants x 3 species: word stores)."""
+    import ctypes as C
+    import torch
+    from cutauleaping_b200 import inputs
+    L = ctl.lib()
+    for net, kw in ((inputs.synthetic(16, 32, 200, seed=7, t_end=0.5, samples=12, perturb_sigma=0.5, perturb_seed=7),
+                     {"group": 4}),
+                    (inputs.schlogl(300, samples=25, t_end=1.0), {})):
+        m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
+        cfg = ctl.run_cfg(seed=21, **kw)
+        hX = torch.from_numpy(np.ascontiguousarray(net.X0, np.int32)).pin_memory()
+        hc = torch.from_numpy(np.ascontiguousarray(net.c, np.float32)).pin_memory()
+        hout = torch.full((net.n, m.ns, m.s_out), -1, dtype=torch.int32).pin_memory()
+        hinfo = torch.zeros((net.n, 40), dtype=torch.uint8).pin_memory()
+        st = L.ctl_run(m.handle, C.byref(cfg), net.n, C.c_void_p(hX.data_ptr()), C.c_void_p(hc.data_ptr()),
+                       C.c_void_p(hout.data_ptr()), C.c_void_p(hinfo.data_ptr()))
+        assert st == ctl.OK, L.ctl_last_error()
+        ref, ref_info = m.run(net.X0, net.c, cfg)          # pageable buffers: copies after the sweep
+        assert np.array_equal(hout.numpy().view(np.uint32), ref)
+        assert np.array_equal(hinfo.numpy(), ref_info.view(np.uint8).reshape(-1, 40))
+
+
 def test_autotune_caches_a_shape_and_keeps_results():
     """ctl_autotune times the library's plan and its candidates, caches the
     winner for this batch size, and later calls with group == threads == 0
