@@ -108,9 +108,13 @@ typedef struct {
     int32_t min_blocks;   /* register budget: kernel variant compiled for this many resident
                              256-thread blocks per SM (2: up to 128 registers per thread,
                              3: 80, 4: 64); 0 = library choice (autotuned, else 3 for
-                             groups of 8+ lanes whose slots fit three blocks, else 2) */
-    int32_t sched;        /* scheduling: 1 = block rounds regrouping simulations by phase,
-                             2 = warp-local (no block barriers); 0 = library choice   */
+                             groups of 8+ lanes whose slots fit three blocks, else 2;
+                             2 for the register-resident sweep, whose kernel compiled for
+                             the network takes the budget given here) */
+    int32_t sched;        /* scheduling: 1 = block rounds regrouping simulations by phase
+                             (the register-resident sweep moves their state through shared
+                             memory), 2 = warp-local (no block barriers; warp lockstep);
+                             0 = library choice                                       */
     int32_t warp_sims;    /* register-resident sweep for tiny networks (at most 16 reactions,
                              8 species and sampled species, 3 reactant entries per reaction),
                              one thread per simulation: simulations per warp, 1..32 (with
