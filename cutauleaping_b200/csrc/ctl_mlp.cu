@@ -36,6 +36,7 @@ struct Gemm {
     const __nv_bfloat16* A;
     const __nv_bfloat16* B;
     int lda, ldb, M, N, K, kt_per_split, epi;
+    int bn;                     // columns of C per CTA (N tile, multiple of 16, <= 256)
     const float* bias;          // [N]
     const float* z_in;          // [M][ldz] pre-activations (SiLU gradient)
     int ldz;
@@ -177,7 +178,7 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(Gemm p) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ uint32_t tmem_slot;
-    const int BN = p.N < 256 ? p.N : 256;
+    const int BN = p.bn;
     const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
     const int ktiles = p.K / BK;
     const int kt0 = blockIdx.z * p.kt_per_split;
@@ -808,7 +809,18 @@ extern "C" ctl_status ctl_mlp_gemm(const ctl_gemm_desc* d, void* stream) {
     const int ktiles = d->K / 64;
     const int splits = d->splits > 0 ? (d->splits < ktiles ? d->splits : ktiles) : 1;
     p.kt_per_split = (ktiles + splits - 1) / splits;
-    const int BN = d->N < 256 ? d->N : 256;
+    // N tile: up to 256 columns, halved (down to 64) while the grid would
+    // leave SMs idle -- each CTA's epilogue (TMEM loads, bias, SiLU, three
+    // stores per element) then covers fewer columns
+    int BN = d->N < 256 ? d->N : 256;
+    static int sm_count = 0;
+    if (!sm_count) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sm_count = 148;
+    }
+    while (BN > 64 && BN % 32 == 0 && (long long)(d->M / 128) * (d->N / BN) * splits < sm_count) BN /= 2;
+    p.bn = BN;
     const size_t smem = (size_t)2 * mlp::BM * mlp::BK * 2 + (size_t)2 * BN * mlp::BK * 2;
     static bool attr_set = false;
     if (!attr_set) {
