@@ -157,6 +157,12 @@ __device__ __forceinline__ float silu_grad(float z) {
     return s * (1.0f + z * (1.0f - s));
 }
 
+// Two FP32 values -> two BF16 (round to nearest even) in one conversion.
+__device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
 // ---- the GEMM -----------------------------------------------------------------
 
 enum { EPI_ATOMIC_F32 = 0, EPI_BIAS_SILU = 1, EPI_BIAS = 2, EPI_SILU_GRAD = 3, EPI_F32 = 4 };
@@ -238,6 +244,34 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(Gemm p) {
     tc_fence_after();
     if (last >= 0 && ok) {
         const int row = m0 + warp * 32 + lane;
+        // A thread holds 8 consecutive columns of its row: it writes them as
+        // 16- and 32-byte vectors (one sector per thread) when the row
+        // strides allow, instead of eight 4-byte stores to 32 rows at a time.
+        const bool vf = (p.ldo & 3) == 0 && (reinterpret_cast<uintptr_t>(p.out_f32) & 15) == 0;
+        const bool vb = (p.ldob & 7) == 0 && (reinterpret_cast<uintptr_t>(p.out_bf) & 15) == 0;
+        auto store_f32 = [&](int n, const float (&o)[8]) {
+            float* dst = p.out_f32 + (size_t)row * p.ldo + n;
+            if (vf) {
+                reinterpret_cast<float4*>(dst)[0] = make_float4(o[0], o[1], o[2], o[3]);
+                reinterpret_cast<float4*>(dst)[1] = make_float4(o[4], o[5], o[6], o[7]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; j++) dst[j] = o[j];
+            }
+        };
+        auto store_bf = [&](int n, const float (&o)[8]) {
+            __nv_bfloat16* dst = p.out_bf + (size_t)row * p.ldob + n;
+            if (vb) {
+                *reinterpret_cast<uint4*>(dst) = make_uint4(pack_bf2(o[0], o[1]), pack_bf2(o[2], o[3]),
+                                                            pack_bf2(o[4], o[5]), pack_bf2(o[6], o[7]));
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; j++) dst[j] = __float2bfloat16(o[j]);
+            }
+            if (p.out_bfT)
+#pragma unroll
+                for (int j = 0; j < 8; j++) p.out_bfT[(size_t)(n + j) * p.ldobT + row] = __float2bfloat16(o[j]);
+        };
         for (int c = 0; c < BN; c += 8) {
             float v[8];
             tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
@@ -246,28 +280,26 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(Gemm p) {
 #pragma unroll
                 for (int j = 0; j < 8; j++) atomicAdd(p.out_f32 + (size_t)row * p.ldo + n + j, v[j]);
             } else if (p.epi == EPI_F32) {
-#pragma unroll
-                for (int j = 0; j < 8; j++) p.out_f32[(size_t)row * p.ldo + n + j] = v[j];
+                store_f32(n, v);
             } else if (p.epi == EPI_BIAS) {
+                float o[8];
 #pragma unroll
-                for (int j = 0; j < 8; j++) p.out_f32[(size_t)row * p.ldo + n + j] = v[j] + p.bias[n + j];
+                for (int j = 0; j < 8; j++) o[j] = v[j] + p.bias[n + j];
+                store_f32(n, o);
             } else if (p.epi == EPI_BIAS_SILU) {
+                float z[8], h[8];
 #pragma unroll
                 for (int j = 0; j < 8; j++) {
-                    const float z = v[j] + p.bias[n + j];
-                    p.out_f32[(size_t)row * p.ldo + n + j] = z;
-                    const __nv_bfloat16 h = __float2bfloat16(silu(z));
-                    p.out_bf[(size_t)row * p.ldob + n + j] = h;
-                    if (p.out_bfT) p.out_bfT[(size_t)(n + j) * p.ldobT + row] = h;
+                    z[j] = v[j] + p.bias[n + j];
+                    h[j] = silu(z[j]);
                 }
+                store_f32(n, z);
+                store_bf(n, h);
             } else {  // EPI_SILU_GRAD
+                float d[8];
 #pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const float z = p.z_in[(size_t)row * p.ldz + n + j];
-                    const __nv_bfloat16 d = __float2bfloat16(v[j] * silu_grad(z));
-                    p.out_bf[(size_t)row * p.ldob + n + j] = d;
-                    if (p.out_bfT) p.out_bfT[(size_t)(n + j) * p.ldobT + row] = d;
-                }
+                for (int j = 0; j < 8; j++) d[j] = v[j] * silu_grad(p.z_in[(size_t)row * p.ldz + n + j]);
+                store_bf(n, d);
             }
         }
     }
@@ -468,11 +500,6 @@ __device__ __forceinline__ uint32_t canon(int row, int k, int rows) {
     return (uint32_t)(((k >> 3) * (rows >> 3) + (row >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
-// Two FP32 values -> two BF16 (round to nearest even) in one conversion.
-__device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
-    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
-    return *reinterpret_cast<const uint32_t*>(&v);
-}
 
 // Layer-0 input columns [32 h, 32 h + 32) of row r of the tile: scaled log
 // parameters in [-1, 1], scaled time, zeros (the same FP32 operations as
@@ -809,17 +836,7 @@ extern "C" ctl_status ctl_mlp_gemm(const ctl_gemm_desc* d, void* stream) {
     const int ktiles = d->K / 64;
     const int splits = d->splits > 0 ? (d->splits < ktiles ? d->splits : ktiles) : 1;
     p.kt_per_split = (ktiles + splits - 1) / splits;
-    // N tile: up to 256 columns, halved (down to 64) while the grid would
-    // leave SMs idle -- each CTA's epilogue (TMEM loads, bias, SiLU, three
-    // stores per element) then covers fewer columns
-    int BN = d->N < 256 ? d->N : 256;
-    static int sm_count = 0;
-    if (!sm_count) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-            sm_count = 148;
-    }
-    while (BN > 64 && BN % 32 == 0 && (long long)(d->M / 128) * (d->N / BN) * splits < sm_count) BN /= 2;
+    const int BN = d->N < 256 ? d->N : 256;
     p.bn = BN;
     const size_t smem = (size_t)2 * mlp::BM * mlp::BK * 2 + (size_t)2 * BN * mlp::BK * 2;
     static bool attr_set = false;
