@@ -280,7 +280,8 @@ def bench_gemm(a):
     """The surrogate's training GEMM alone (ctl_mlp_gemm, tcgen05): the
     hidden-layer forward product of a 16,384-row training batch (M = 16384,
     N = K = 256, bias + SiLU epilogue writing FP32 and BF16) and its weight
-    gradient (M = N = 256, K = 16384, split-K 8, FP32 atomic epilogue); 2MNK
+    gradient (M = N = 256, K = 16384, split-K 32 as training takes it:
+    batch / 512, at most 64; FP32 atomic epilogue); 2MNK
     FLOPs per launch, CUDA events on the launching stream over 20 launches
     after 5 warm-ups; peak = the measured burst BF16 GEMM rate."""
     import torch
@@ -300,8 +301,8 @@ def bench_gemm(a):
     shapes = {
         "forward (M=16384, N=256, K=256, bias+SiLU)": (lambda: sg.gemm(X, Wt, epilogue=sg.EPI_BIAS_SILU, out_f32=z,
                                                                       out_bf=h, bias=bias, err=err), B * W * W),
-        "weight gradient (M=256, N=256, K=16384, split-K 8)": (lambda: sg.gemm(XT, XT, epilogue=sg.EPI_ATOMIC_F32,
-                                                                              out_f32=dW, splits=8, err=err), W * W * B),
+        "weight gradient (M=256, N=256, K=16384, split-K 32)": (lambda: sg.gemm(XT, XT, epilogue=sg.EPI_ATOMIC_F32,
+                                                                               out_f32=dW, splits=32, err=err), W * W * B),
     }
     out = {}
     for name, (fn, mnk) in shapes.items():
