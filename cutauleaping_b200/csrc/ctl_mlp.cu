@@ -19,6 +19,7 @@
 // instead of hanging.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cstdint>
 #include <algorithm>
@@ -180,6 +181,71 @@ __device__ __forceinline__ void stage_tile(uint8_t* dst, const __nv_bfloat16* sr
     }
 }
 
+// The epilogue: warp w reads TMEM lanes 32w..32w+31 (rows m0 + 32w + lane),
+// 8 columns at a time, and applies the descriptor's epilogue.
+__device__ __forceinline__ void gemm_epilogue(const Gemm& p, uint32_t tmem, int BN, int m0, int n0, int warp,
+                                              int lane) {
+    const int row = m0 + warp * 32 + lane;
+    // A thread holds 8 consecutive columns of its row: it writes them as
+    // 16- and 32-byte vectors (one sector per thread) when the row
+    // strides allow, instead of eight 4-byte stores to 32 rows at a time.
+    const bool vf = (p.ldo & 3) == 0 && (reinterpret_cast<uintptr_t>(p.out_f32) & 15) == 0;
+    const bool vb = (p.ldob & 7) == 0 && (reinterpret_cast<uintptr_t>(p.out_bf) & 15) == 0;
+    auto store_f32 = [&](int n, const float (&o)[8]) {
+        float* dst = p.out_f32 + (size_t)row * p.ldo + n;
+        if (vf) {
+            reinterpret_cast<float4*>(dst)[0] = make_float4(o[0], o[1], o[2], o[3]);
+            reinterpret_cast<float4*>(dst)[1] = make_float4(o[4], o[5], o[6], o[7]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; j++) dst[j] = o[j];
+        }
+    };
+    auto store_bf = [&](int n, const float (&o)[8]) {
+        __nv_bfloat16* dst = p.out_bf + (size_t)row * p.ldob + n;
+        if (vb) {
+            *reinterpret_cast<uint4*>(dst) = make_uint4(pack_bf2(o[0], o[1]), pack_bf2(o[2], o[3]),
+                                                        pack_bf2(o[4], o[5]), pack_bf2(o[6], o[7]));
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; j++) dst[j] = __float2bfloat16(o[j]);
+        }
+        if (p.out_bfT)
+#pragma unroll
+            for (int j = 0; j < 8; j++) p.out_bfT[(size_t)(n + j) * p.ldobT + row] = __float2bfloat16(o[j]);
+    };
+    for (int c = 0; c < BN; c += 8) {
+        float v[8];
+        tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+        const int n = n0 + c;
+        if (p.epi == EPI_ATOMIC_F32) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) atomicAdd(p.out_f32 + (size_t)row * p.ldo + n + j, v[j]);
+        } else if (p.epi == EPI_F32) {
+            store_f32(n, v);
+        } else if (p.epi == EPI_BIAS) {
+            float o[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) o[j] = v[j] + p.bias[n + j];
+            store_f32(n, o);
+        } else if (p.epi == EPI_BIAS_SILU) {
+            float z[8], h[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                z[j] = v[j] + p.bias[n + j];
+                h[j] = silu(z[j]);
+            }
+            store_f32(n, z);
+            store_bf(n, h);
+        } else {  // EPI_SILU_GRAD
+            float d[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) d[j] = v[j] * silu_grad(p.z_in[(size_t)row * p.ldz + n + j]);
+            store_bf(n, d);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(Gemm p) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(8) uint64_t bars[2];
@@ -242,67 +308,114 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(Gemm p) {
     if (last >= 0 && ok) ok = mbar_wait(&bars[last], par[last], p.err);
     ok = __syncthreads_and(ok) != 0;  // tcgen05.ld below is warp-collective
     tc_fence_after();
-    if (last >= 0 && ok) {
-        const int row = m0 + warp * 32 + lane;
-        // A thread holds 8 consecutive columns of its row: it writes them as
-        // 16- and 32-byte vectors (one sector per thread) when the row
-        // strides allow, instead of eight 4-byte stores to 32 rows at a time.
-        const bool vf = (p.ldo & 3) == 0 && (reinterpret_cast<uintptr_t>(p.out_f32) & 15) == 0;
-        const bool vb = (p.ldob & 7) == 0 && (reinterpret_cast<uintptr_t>(p.out_bf) & 15) == 0;
-        auto store_f32 = [&](int n, const float (&o)[8]) {
-            float* dst = p.out_f32 + (size_t)row * p.ldo + n;
-            if (vf) {
-                reinterpret_cast<float4*>(dst)[0] = make_float4(o[0], o[1], o[2], o[3]);
-                reinterpret_cast<float4*>(dst)[1] = make_float4(o[4], o[5], o[6], o[7]);
-            } else {
+    if (last >= 0 && ok) gemm_epilogue(p, tmem, BN, m0, n0, warp, lane);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
+// ---- the GEMM with TMA tile loads -------------------------------------------------
+//
+// The same product, with the operand tiles brought into shared memory by
+// the tensor-memory accelerator instead of through registers: thread 0
+// issues, per K tile, eight 2D bulk tensor loads of A (box 8 elements x 128
+// rows) and eight of B (8 x BN) -- each lands as one column of 8-row x
+// 16-byte core matrices, which is exactly the canonical no-swizzle K-major
+// layout -- completing on the stage's full mbarrier; the same thread issues
+// that tile's MMAs once the stage is full and refills the stage when the
+// MMAs reading it have completed (tcgen05.commit on its empty mbarrier).
+// Four stages hold a 256-deep K slice of a 128 x 256 tile.  The tensor maps
+// cover the operands in this GPU's own memory; no multicast.
+
+constexpr int TMA_STAGES = 4;
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+    gemm_tma_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, Gemm p) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t full[TMA_STAGES], empty[TMA_STAGES];
+    __shared__ uint32_t tmem_slot;
+    const int BN = p.bn;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int ktiles = p.K / BK;
+    const int kt0 = blockIdx.z * p.kt_per_split;
+    const int kt1 = min(kt0 + p.kt_per_split, ktiles);
+    const int nk = kt1 > kt0 ? kt1 - kt0 : 0;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const uint32_t a_bytes = BM * BK * 2, stage_bytes = (uint32_t)(BM + BN) * BK * 2;
+    uint32_t ncols = 32;
+    while ((int)ncols < BN) ncols <<= 1;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TMA_STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_slot)), "r"(ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    bool ok = true;
+    if (threadIdx.x == 0 && nk > 0) {
+        const uint32_t idesc = make_idesc(BM, BN);
+        auto issue = [&](int i, int s) {
+            uint8_t* sa = smem + (size_t)s * stage_bytes;
+            uint8_t* sb = sa + a_bytes;
+            const int kx = (kt0 + i) * BK;
+            mbar_expect(&full[s], stage_bytes);
 #pragma unroll
-                for (int j = 0; j < 8; j++) dst[j] = o[j];
+            for (int kb = 0; kb < BK / 8; kb++) {
+                tma_load_2d(sa + kb * BM * 16, &ta, kx + kb * 8, m0, &full[s]);
+                tma_load_2d(sb + kb * BN * 16, &tb, kx + kb * 8, n0, &full[s]);
             }
         };
-        auto store_bf = [&](int n, const float (&o)[8]) {
-            __nv_bfloat16* dst = p.out_bf + (size_t)row * p.ldob + n;
-            if (vb) {
-                *reinterpret_cast<uint4*>(dst) = make_uint4(pack_bf2(o[0], o[1]), pack_bf2(o[2], o[3]),
-                                                            pack_bf2(o[4], o[5]), pack_bf2(o[6], o[7]));
-            } else {
+        const int pre = nk < TMA_STAGES ? nk : TMA_STAGES;
+        for (int i = 0; i < pre; i++) issue(i, i);
+        for (int i = 0; i < nk && ok; i++) {
+            const int s = i % TMA_STAGES;
+            const uint32_t ph = (uint32_t)(i / TMA_STAGES) & 1u;
+            ok = mbar_wait(&full[s], ph, p.err);
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t a = smem_u32(smem + (size_t)s * stage_bytes), b = a + a_bytes;
 #pragma unroll
-                for (int j = 0; j < 8; j++) dst[j] = __float2bfloat16(o[j]);
+            for (int kk = 0; kk < BK / 16; kk++) {
+                const uint64_t da = make_desc(a + kk * 2 * (BM / 8) * 128, (BM / 8) * 128, 128);
+                const uint64_t db = make_desc(b + kk * 2 * (BN / 8) * 128, (BN / 8) * 128, 128);
+                mma_bf16(tmem, da, db, idesc, (i > 0 || kk > 0) ? 1u : 0u);
             }
-            if (p.out_bfT)
-#pragma unroll
-                for (int j = 0; j < 8; j++) p.out_bfT[(size_t)(n + j) * p.ldobT + row] = __float2bfloat16(o[j]);
-        };
-        for (int c = 0; c < BN; c += 8) {
-            float v[8];
-            tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-            const int n = n0 + c;
-            if (p.epi == EPI_ATOMIC_F32) {
-#pragma unroll
-                for (int j = 0; j < 8; j++) atomicAdd(p.out_f32 + (size_t)row * p.ldo + n + j, v[j]);
-            } else if (p.epi == EPI_F32) {
-                store_f32(n, v);
-            } else if (p.epi == EPI_BIAS) {
-                float o[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) o[j] = v[j] + p.bias[n + j];
-                store_f32(n, o);
-            } else if (p.epi == EPI_BIAS_SILU) {
-                float z[8], h[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    z[j] = v[j] + p.bias[n + j];
-                    h[j] = silu(z[j]);
-                }
-                store_f32(n, z);
-                store_bf(n, h);
-            } else {  // EPI_SILU_GRAD
-                float d[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) d[j] = v[j] * silu_grad(p.z_in[(size_t)row * p.ldz + n + j]);
-                store_bf(n, d);
+            mma_commit(&empty[s]);
+            if (i + TMA_STAGES < nk) {  // the stage is free once these MMAs completed
+                ok = mbar_wait(&empty[s], ph, p.err);
+                if (ok) issue(i + TMA_STAGES, s);
             }
         }
+        // every MMA has completed once the last commit arrived
+        if (ok) {
+            const int l = nk - 1;
+            ok = mbar_wait(&empty[l % TMA_STAGES], (uint32_t)(l / TMA_STAGES) & 1u, p.err);
+        }
     }
+    ok = __syncthreads_and(ok) != 0;  // tcgen05.ld below is warp-collective
+    tc_fence_after();
+    if (nk > 0 && ok) gemm_epilogue(p, tmem, BN, m0, n0, warp, lane);
     tc_fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
@@ -782,6 +895,32 @@ static ctl_status mlp_cuda(cudaError_t e, const char* what) {
 namespace ctl {
 namespace mlp {
 
+// A 2D tensor map over a row-major BF16 operand [rows][ld] (K contiguous)
+// with boxes of 8 K-elements x box_rows rows, for gemm_tma_kernel.  False
+// when the driver offers no encoder or the operand breaks its rules.
+static bool tensor_map(CUtensorMap& map, const void* base, int K, int rows, int ld, int box_rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        else
+            cudaGetLastError();
+        tried = true;
+    }
+    if (!encode || (reinterpret_cast<uintptr_t>(base) & 15) || ((size_t)ld * 2) % 16 || box_rows > 256) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1u, 1u};
+    return encode(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // One warp waits, through the same bounded wait as the GEMM and screening
 // kernels, on an mbarrier that nothing arrives on; no MMA or bulk copy is in
 // flight.  The wait gives up after `limit` polls, raises bit 0 of *err and
@@ -848,6 +987,23 @@ extern "C" ctl_status ctl_mlp_gemm(const ctl_gemm_desc* d, void* stream) {
         attr_set = true;
     }
     dim3 grid((unsigned)(d->M / 128), (unsigned)((d->N + BN - 1) / BN), (unsigned)splits);
+    // TMA tile loads when the driver's tensor-map encoder is available and
+    // the operands meet its rules (16-byte aligned bases and row strides);
+    // register staging otherwise.
+    CUtensorMap ta, tb;
+    if (mlp::tensor_map(ta, d->A, d->K, d->M, d->lda, 128) && mlp::tensor_map(tb, d->B, d->K, d->N, d->ldb, BN)) {
+        const size_t tsmem = (size_t)mlp::TMA_STAGES * (size_t)(mlp::BM + BN) * mlp::BK * 2;
+        static bool tattr_set = false;
+        if (!tattr_set) {
+            ctl_status st = mlp_cuda(cudaFuncSetAttribute(mlp::gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                          mlp::TMA_STAGES * (mlp::BM + 256) * mlp::BK * 2),
+                                     "cudaFuncSetAttribute(gemm_tma)");
+            if (st != CTL_OK) return st;
+            tattr_set = true;
+        }
+        mlp::gemm_tma_kernel<<<grid, mlp::THREADS, tsmem, static_cast<cudaStream_t>(stream)>>>(ta, tb, p);
+        return mlp_cuda(cudaGetLastError(), "gemm_tma_kernel launch");
+    }
     mlp::gemm_kernel<<<grid, mlp::THREADS, smem, static_cast<cudaStream_t>(stream)>>>(p);
     return mlp_cuda(cudaGetLastError(), "gemm_kernel launch");
 }
