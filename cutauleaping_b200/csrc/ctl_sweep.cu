@@ -506,7 +506,7 @@ static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_
             ws = (int)std::min<uint64_t>(8, std::max<uint64_t>(1, per));
         }
         const uint64_t slots = (uint64_t)ws * wpb;
-        smem = (size_t)(2 * pl.tinySM + 18) * (size_t)threads * 4;
+        smem = (size_t)(2 * pl.tinySM + 20 + pl.tinyP) * (size_t)threads * 4;  // Packed<P, SM>::WORDS
         need = ((uint64_t)n + slots - 1) / slots;
     } else {
         if (ws <= 0) {

@@ -128,14 +128,20 @@ struct Sim {
     uint32_t pre;
     double pre_u;
     float pre_lg;
+    uint4 wc;         // Philox block of SSA steps 2 wc_blk, 2 wc_blk + 1 (not carried across rounds)
+    uint32_t wc_blk;
 };
 
 // Pick uniform and waiting-time log of SSA step `step`: one Philox block per
 // two steps, (w0, w1) for even steps and (w2, w3) for odd ones, as
-// dev::ssa_step.
-__device__ __forceinline__ void ssa_randoms(const dev::Run& run, uint32_t simg, uint32_t step, double& u, float& lg) {
-    const uint4 w = dev::draw(run.seed, 0u, dev::TAG_SSA, step >> 1, simg);
-    const uint32_t wa = (step & 1u) ? w.z : w.x, wb = (step & 1u) ? w.w : w.y;
+// dev::ssa_step; the block is kept for the pair's second step.
+__device__ __forceinline__ void ssa_randoms(const dev::Run& run, uint32_t simg, uint32_t step, Sim& st, double& u,
+                                            float& lg) {
+    if (st.wc_blk != (step >> 1)) {
+        st.wc = dev::draw(run.seed, 0u, dev::TAG_SSA, step >> 1, simg);
+        st.wc_blk = step >> 1;
+    }
+    const uint32_t wa = (step & 1u) ? st.wc.z : st.wc.x, wb = (step & 1u) ? st.wc.w : st.wc.y;
     u = dev::u32d(wa);
     lg = dev::flog(dev::u24f(wb));
 }
@@ -403,9 +409,13 @@ __device__ __forceinline__ int ssa_step(const N& net, const dev::Run& run, State
         u = st.pre_u;
         lg = st.pre_lg;
     } else {
-        ssa_randoms(run, simg, step, u, lg);
+        ssa_randoms(run, simg, step, st, u, lg);
     }
     const int r = descend<P>(s.t, u * A0);
+    // the next step's random part, free of the state (a leap decision in
+    // between leaves it unused)
+    ssa_randoms(run, simg, step + 1u, st, st.pre_u, st.pre_lg);
+    st.pre = step + 1u;
     const float dtf = -lg / (float)A0;
     st.tl = st.tl + (double)dtf;
     while (st.cursor < ns && st.T + st.tl > st.t_next) {
@@ -431,12 +441,8 @@ __device__ __forceinline__ int ssa_step(const N& net, const dev::Run& run, State
     }
     st.ssa++;
     st.fire += 1ull;
-    // Straight-line from the update to the new sum tree, with the next step's
-    // random part (free of the state; a leap decision in between leaves it
-    // unused) in the same block so that it fills the tree chain's stalls.
-    // After an overflow the propensities are computed and discarded.
-    ssa_randoms(run, simg, step + 1u, st.pre_u, st.pre_lg);
-    st.pre = step + 1u;
+    // straight-line from the update to the new sum tree (after an overflow
+    // the propensities are computed and discarded)
     all_props<N, P, SM>(net, s);
     if (ovf) { st.status = CTL_SIM_OVERFLOW; return DONE; }
     st.burst++;
@@ -500,6 +506,7 @@ __device__ __forceinline__ void start_sim(const N& net, const dev::Run& run, Sta
     st.status = CTL_SIM_OK;
     st.in_ssa = (run.flags & dev::F_FORCE_SSA) != 0;
     st.pre = 0xffffffffu;
+    st.wc_blk = 0xffffffffu;
 }
 
 template <class N>
@@ -588,21 +595,23 @@ __device__ __forceinline__ void sweep(const N& net, const dev::Run& run, uint32_
 }
 
 // Words of one simulation's resumable state in the regrouping exchange:
-// populations, the time and counters, the prepared random part of the next
-// SSA step and (fitness mode) the last recorded sample.  Rate constants,
-// propensities and the sum tree are rebuilt from them.
-template <int SM>
+// populations, the time and counters, the next sample instant, the prepared
+// random part of the next SSA step, (fitness mode) the last recorded sample
+// and the rate constants.  Propensities and the sum tree are rebuilt from
+// them.
+template <int P, int SM>
 struct Packed {
     static constexpr int X = 0, T = SM, TL = SM + 2, FIRE = SM + 4, SIM = SM + 6, CURSOR = SM + 7, NSTEP = SM + 8,
                          BURST = SM + 9, LEAPS = SM + 10, SSA = SM + 11, REJ = SM + 12, FLAGS = SM + 13,
-                         PRE = SM + 14, PREU = SM + 15, PRELG = SM + 17, LAST = SM + 18, WORDS = 2 * SM + 18;
+                         PRE = SM + 14, PREU = SM + 15, PRELG = SM + 17, TNEXT = SM + 18, LAST = SM + 20,
+                         C = 2 * SM + 20, WORDS = 2 * SM + 20 + P;
 };
 
 // Word w of slot j: structure of arrays, consecutive slots in consecutive banks.
 template <int P, int SM>
 __device__ __forceinline__ void put_state(uint32_t* xs, uint32_t ns, uint32_t j, const State<P, SM>& s,
                                           const Sim& st) {
-    using K = Packed<SM>;
+    using K = Packed<P, SM>;
     auto w = [&](int i, uint32_t v) { xs[(uint32_t)i * ns + j] = v; };
     auto w64 = [&](int i, unsigned long long v) {
         w(i, (uint32_t)v);
@@ -627,12 +636,15 @@ __device__ __forceinline__ void put_state(uint32_t* xs, uint32_t ns, uint32_t j,
     w(K::PRE, st.pre);
     w64(K::PREU, (unsigned long long)__double_as_longlong(st.pre_u));
     w(K::PRELG, __float_as_uint(st.pre_lg));
+    w64(K::TNEXT, (unsigned long long)__double_as_longlong(st.t_next));
+#pragma unroll
+    for (int r = 0; r < P; r++) w(K::C + r, __float_as_uint(s.c[r]));
 }
 
 template <class N, int P, int SM>
 __device__ __forceinline__ void get_state(const N& net, const uint32_t* xs, uint32_t ns, uint32_t j, State<P, SM>& s,
                                           Sim& st) {
-    using K = Packed<SM>;
+    using K = Packed<P, SM>;
     auto r = [&](int i) { return xs[(uint32_t)i * ns + j]; };
     auto r64 = [&](int i) { return (unsigned long long)r(i) | ((unsigned long long)r(i + 1) << 32); };
 #pragma unroll
@@ -656,7 +668,10 @@ __device__ __forceinline__ void get_state(const N& net, const uint32_t* xs, uint
     st.pre = r(K::PRE);
     st.pre_u = __longlong_as_double((long long)r64(K::PREU));
     st.pre_lg = __uint_as_float(r(K::PRELG));
-    st.t_next = st.cursor < (uint32_t)net.ns() ? net.tvec()[st.cursor] : 0.0;
+    st.t_next = __longlong_as_double((long long)r64(K::TNEXT));
+    st.wc_blk = 0xffffffffu;
+#pragma unroll
+    for (int q = 0; q < P; q++) s.c[q] = __uint_as_float(r(K::C + q));
 }
 
 // Block rounds with regrouping: at most `slots` simulations live in a block
@@ -668,8 +683,8 @@ __device__ __forceinline__ void get_state(const N& net, const uint32_t* xs, uint
 // each warp runs one phase only (with slots <= 32 in a 64-thread block, warp
 // 0 steps SSA while warp 1 decides).  Then SSA threads take up to ssa_budget
 // steps and deciding threads up to dec_budget decisions, and the block meets
-// at a barrier.  xs: dynamic shared memory of Packed<SM>::WORDS words per
-// thread.
+// at a barrier.  xs: dynamic shared memory of Packed<P, SM>::WORDS words
+// per thread.
 template <class N, int P, int SM>
 __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, uint32_t slots, uint32_t* xs) {
     __shared__ uint32_t s_cnt[2][32];
@@ -735,7 +750,7 @@ __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, 
         live = mine_ssa || mine_dec;
         if (live) {
             get_state<N, P, SM>(net, xs, nt, tid, s, st);
-            load_rates<N, P, SM>(net, run, s, st.sim);
+            all_props<N, P, SM>(net, s);
             o = out_for(run, st.sim, row_words);
         }
         const uint32_t smask = __ballot_sync(0xffffffffu, mine_ssa);
