@@ -477,13 +477,13 @@ static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_
     pl.tinySM = tiny_species_bound(t);
     // register budget of the compiled kernel (the library's own is built for 2)
     const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : 2;
-    pl.spec = cfg->tiny_spec >= 0 ? tiny_spec_kernel(t, cfg->flags, minb, nullptr) : nullptr;
+    const int sched = cfg->sched > 0 ? cfg->sched : TINY_DEFAULT_SCHED;
+    pl.spec = cfg->tiny_spec >= 0 ? tiny_spec_kernel(t, cfg->flags, minb, sched, nullptr) : nullptr;
     const void* k = pl.spec ? pl.spec : tiny_kernel_ptr(pl.tinyP, pl.tinySM);
     if (!k) {
         set_error("no register-resident kernel for this network");
         return CTL_ERR_SHAPE;
     }
-    const int sched = cfg->sched > 0 ? cfg->sched : TINY_DEFAULT_SCHED;
     int threads = cfg->threads > 0 ? cfg->threads : (sched == 1 ? 64 : 256);
     if (threads % 32 || threads < 32 || threads > 256 || (sched == 1 && threads < 64)) {
         set_error("threads per block must be a multiple of 32, at most 256 (at least 64 for block rounds)");
@@ -522,9 +522,22 @@ static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_
         if (cfg->threads <= 0 && warps <= (uint64_t)da.sm_count * 8) threads = 64;
         need = (warps * 32 + threads - 1) / threads;
     }
+    if (smem > (size_t)da.smem_optin) {
+        set_error("register-resident sweep: the block-round exchange needs more shared memory than a block has");
+        return CTL_ERR_SHAPE;
+    }
     int bps = 0, regs = 0;
     {
         std::lock_guard<std::mutex> lk(g_attr_mu);
+        if (smem > 48 * 1024) {  // above the default dynamic limit: raise the kernel's ceiling once
+            static std::vector<std::pair<int, const void*>> raised;
+            bool done = false;
+            for (const auto& r : raised) done = done || (r.first == cfg->device && r.second == k);
+            if (!done) {
+                CTL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, da.smem_optin));
+                raised.push_back({cfg->device, k});
+            }
+        }
         for (const auto& o : g_tiny_occ)
             if (o.dev == cfg->device && o.kernel == k && o.threads == threads && o.smem == smem) {
                 bps = o.bps;

@@ -199,7 +199,7 @@ void accessor(std::ostringstream& o, const char* decl, int rows, int cols, F&& v
     o << " default: return 0; } }\n";
 }
 
-std::string spec_source(const HostTables& t, uint32_t flags, int minb) {
+std::string spec_source(const HostTables& t, uint32_t flags, int minb, int sched) {
     tiny::Net n;
     tiny_net(t, flags, nullptr, n);
     const int P = t.P, SM = tiny_species_bound(t);
@@ -223,9 +223,14 @@ std::string spec_source(const HostTables& t, uint32_t flags, int minb) {
     accessor(o, "unsigned cs(int a, int b = 0)", tiny::MAX_S, 1, [&](int i, int) { return (long long)n.cs[i]; });
     accessor(o, "unsigned frow(int a, int b)", tiny::MAX_R, 2, [&](int i, int j) { return (long long)n.frow[i][j]; });
     o << "};\n";
+    // one schedule per kernel: warp lockstep (2) or block rounds (1)
     o << "extern \"C\" __global__ void __launch_bounds__(256, " << minb << ") ctl_tiny_spec("
-         "const __grid_constant__ NetCT net, const __grid_constant__ ctl::dev::Run run, unsigned lanes) {\n"
-         "    ctl::tiny::run_sweep<NetCT, " << P << ", " << SM << ">(net, run, lanes);\n}\n";
+         "const __grid_constant__ NetCT net, const __grid_constant__ ctl::dev::Run run, unsigned lanes) {\n";
+    if (sched == 2)
+        o << "    ctl::tiny::sweep<NetCT, " << P << ", " << SM << ">(net, run, lanes);\n}\n";
+    else
+        o << "    extern __shared__ unsigned ctl_tiny_xs[];\n"
+             "    ctl::tiny::sweep_rounds<NetCT, " << P << ", " << SM << ">(net, run, lanes, ctl_tiny_xs);\n}\n";
     return o.str();
 }
 
@@ -280,8 +285,8 @@ const void* compile_spec(const std::string& src, std::string& why) {
 
 }  // namespace
 
-const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, int minb, std::string* why) {
-    const std::string src = spec_source(t, flags & dev::F_Q5_OFF, minb);
+const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, int minb, int sched, std::string* why) {
+    const std::string src = spec_source(t, flags & dev::F_Q5_OFF, minb, sched);
     std::lock_guard<std::mutex> lk(g_spec_mu);
     for (const auto& e : g_spec)
         if (e.source == src) {

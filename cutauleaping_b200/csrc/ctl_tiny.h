@@ -52,9 +52,10 @@ struct SpecNet {
 };
 // The kernel compiled for this network and tau1 table (quirk Q5 in flags)
 // by NVRTC, for minb resident 256-thread blocks per SM (its register
-// budget: 2, 3 or 4), or nullptr when NVRTC is missing or the compilation
-// failed (the reason in *why).  Compiled once per process, network and
-// budget; takes a lock.
-const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, int minb, std::string* why);
+// budget: 2, 3 or 4) and one schedule (1 block rounds, 2 warp lockstep), or
+// nullptr when NVRTC is missing or the compilation failed (the reason in
+// *why).  Compiled once per process, network, budget and schedule; takes a
+// lock.
+const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, int minb, int sched, std::string* why);
 
 }  // namespace ctl
