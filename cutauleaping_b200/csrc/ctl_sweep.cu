@@ -534,7 +534,15 @@ static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_
             bool done = false;
             for (const auto& r : raised) done = done || (r.first == cfg->device && r.second == k);
             if (!done) {
-                CTL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, da.smem_optin));
+                cudaFuncAttributes fa;
+                CTL_CUDA(cudaFuncGetAttributes(&fa, k));
+                if (smem + fa.sharedSizeBytes > (size_t)da.smem_optin) {
+                    set_error("register-resident sweep: the block-round exchange needs more shared memory than a "
+                              "block has");
+                    return CTL_ERR_SHAPE;
+                }
+                CTL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              da.smem_optin - (int)fa.sharedSizeBytes));
                 raised.push_back({cfg->device, k});
             }
         }
