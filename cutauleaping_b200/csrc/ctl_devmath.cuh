@@ -69,6 +69,9 @@ struct Run {
     uint32_t uniform_c;              // all simulations share row 0 of c
     uint32_t ssa_budget, dec_budget; // work per slot and round (SSA steps / decisions)
     uint32_t warp_local;             // 1: warp-local scheduling (no block rounds)
+    uint32_t tail_sims;              // register-resident block rounds: live simulations at or
+                                     // below which a block with a closed queue finishes them in
+                                     // warp lockstep (0: never)
     unsigned long long* sums;        // fitness mode: [sets][ns][s_out] sample sums, else null
     uint32_t sum_threads, sum_prep;  // simulation -> parameter set (the reference's layout)
     uint32_t* done;                  // optional: finished simulations per chunk of 2^done_shift

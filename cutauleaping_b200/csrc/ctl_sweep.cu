@@ -469,14 +469,23 @@ static std::vector<TinyOcc> g_tiny_occ;
 
 // Scheduling of the register-resident sweep when the caller does not choose.
 static constexpr int TINY_DEFAULT_SCHED = 1;
+// Block rounds: a block whose queue is closed finishes a lone simulation in
+// warp lockstep (Schlogl's slowest simulation alone: 6.6 ms against 8.8 ms
+// in rounds); with 2 or more the rounds keep their advantage (16,384
+// simulations: 538k sims/s with 2, 551k with 1, 555k with none).
+static constexpr uint32_t TINY_TAIL_SIMS = 1;
 
 static ctl_status plan_tiny(const HostTables& t, const ctl_run_cfg* cfg, uint32_t n, LaunchPlan& pl) {
     DevAttr da;
     if (device_attr(cfg->device, da) != CTL_OK) return CTL_ERR_CUDA;
     pl.tinyP = t.P;
     pl.tinySM = tiny_species_bound(t);
-    // register budget of the compiled kernel (the library's own is built for 2)
-    const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : 2;
+    // register budget of the kernel compiled for the network (the library's
+    // own is built for 2): 1 by default, which leaves the Schlogl kernels
+    // unspilled (254 registers for block rounds, 187 for warp lockstep,
+    // against 128 with spills at 2) -- 4,096 simulations on one B200: 330k
+    // against 295k sims/s; 65,536: 722k against 650k
+    const int minb = cfg->min_blocks > 0 ? cfg->min_blocks : 1;
     const int sched = cfg->sched > 0 ? cfg->sched : TINY_DEFAULT_SCHED;
     pl.spec = cfg->tiny_spec >= 0 ? tiny_spec_kernel(t, cfg->flags, minb, sched, nullptr) : nullptr;
     const void* k = pl.spec ? pl.spec : tiny_kernel_ptr(pl.tinyP, pl.tinySM);
@@ -606,6 +615,10 @@ static ctl_status plan_launch(ctl_model* m, const ctl_run_cfg* cfg_in, uint32_t 
     }
     if (tiny_ok && (cfg->warp_sims > 0 || (cfg->warp_sims == 0 && cfg->group <= 0)))
         return plan_tiny(t, cfg, n, pl);
+    if (cfg->min_blocks == 1) {
+        set_error("min_blocks 1 applies to the register-resident sweep only; the shared-memory sweep takes 2, 3 or 4");
+        return CTL_ERR_ARG;
+    }
     pl.ssa_budget = cfg->ssa_budget;
     pl.dec_budget = cfg->dec_budget;
     pl.sched = cfg->sched > 0 ? cfg->sched : 1;
@@ -708,6 +721,7 @@ static ctl_status enqueue_sweep(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n
     run.ssa_budget = (uint32_t)pl.ssa_budget;
     run.dec_budget = (uint32_t)pl.dec_budget;
     run.warp_local = pl.sched == 2 ? 1u : 0u;
+    run.tail_sims = TINY_TAIL_SIMS;
     run.X0 = dX0;
     run.c = dc;
     run.out = dout;
@@ -775,8 +789,8 @@ static ctl_status check_cfg(const ctl_run_cfg* cfg) {
         set_error("ssa_steps must be positive");
         return CTL_ERR_ARG;
     }
-    if (cfg->min_blocks != 0 && (cfg->min_blocks < 2 || cfg->min_blocks > 4)) {
-        set_error("min_blocks must be 0 (library choice), 2, 3 or 4");
+    if (cfg->min_blocks != 0 && (cfg->min_blocks < 1 || cfg->min_blocks > 4)) {
+        set_error("min_blocks must be 0 (library choice), 1 (register-resident sweep only), 2, 3 or 4");
         return CTL_ERR_ARG;
     }
     if (cfg->sched < 0 || cfg->sched > 2) {
@@ -1059,7 +1073,7 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         c.threads = x.threads;
         c.ssa_budget = x.ssa;
         c.dec_budget = x.dec;
-        c.min_blocks = x.ws > 0 ? 0 : x.minb;
+        c.min_blocks = x.minb;
         c.sched = x.sched;
         c.warp_sims = x.ws;
         LaunchPlan pl;
@@ -1088,9 +1102,9 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         consider(bestx);                                       // 0. the library's own plan
         if (tiny_eligible(t)) {                                // 1a. register-resident sweep
             for (int ws : {1, 2, 4, 8, 16, 32})                //     warp lockstep
-                if (!(ws == p0.warp_sims && p0.sched == 2)) consider({1, 0, S0 > 0 ? S0 : 16, 1, 2, 2, ws});
+                if (!(ws == p0.warp_sims && p0.sched == 2)) consider({1, 0, S0 > 0 ? S0 : 16, 1, 1, 2, ws});
             for (int ws : {4, 8, 12, 16})                      //     block rounds with regrouping
-                if (!(ws == p0.warp_sims && p0.sched == 1)) consider({1, 0, S0 > 0 ? S0 : 16, 1, 2, 1, ws});
+                if (!(ws == p0.warp_sims && p0.sched == 1)) consider({1, 0, S0 > 0 ? S0 : 16, 2, 1, 1, ws});
         }
         for (int G = 1; G <= 256 && G <= t.P; G <<= 1)        // 1b. lanes per simulation
             if (G != p0.G || p0.warp_sims > 0) consider({G, 256, S0, default_dec_budget(G), 2, 1, -1});
@@ -1104,11 +1118,13 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
             Shape x = bestx;                                   // 3. scheduling: warp-local vs block rounds
             x.sched = bestx.sched == 2 ? 1 : 2;
             consider(x);
-            const Shape b3 = bestx;
-            for (int mb : {2, 3, 4}) {                         // 4. register budget (resident blocks)
+        }
+        {
+            const Shape b3 = bestx;                            // 4. register budget (resident blocks); the
+            for (int mb : {1, 2, 3, 4}) {                      //    register-resident kernel takes 1 or 2
                 Shape y = b3;
                 y.minb = mb;
-                if (mb != b3.minb) consider(y);
+                if (mb != b3.minb && (b3.ws > 0 ? mb <= 2 : mb >= 2)) consider(y);
             }
         }
         const Shape b4 = bestx;
@@ -1138,7 +1154,7 @@ extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_
         std::lock_guard<std::mutex> lk(m->mu);
         const uint32_t nb = n_bucket(n), uni = (uint32_t)(cfg->uniform_rates != 0);
         const ctl_model::Tuned tu{cfg->device, nb, uni, cfg->flags, bestx.ws > 0 ? 0 : bestx.G, bestx.threads,
-                                  bestx.ssa, bestx.dec, bestx.ws > 0 ? 0 : bestx.minb, bestx.sched, bestx.ws};
+                                  bestx.ssa, bestx.dec, bestx.minb, bestx.sched, bestx.ws};
         bool found = false;
         for (auto& x : m->tuned)
             if (x.device == cfg->device && x.nbucket == nb && x.uniform == uni && x.flags == cfg->flags) {

@@ -548,22 +548,17 @@ __device__ __forceinline__ void finish(const N& net, const dev::Run& run, const 
     }
 }
 
-// Warp lockstep: one thread per simulation, `lanes` simulations per warp
-// (lanes 0..lanes-1 of every warp work, the rest exit), simulations pulled
-// from the device work queue.  The working lanes of a warp take their SSA
-// steps and their leap decisions in lockstep phases (up to ssa_budget SSA
-// steps, then up to dec_budget decisions) so that their instruction streams
-// stay merged; a lane in one phase waits while the others run the other.
+// Warp lockstep over the lanes of `mask`: each lane steps its simulation (if
+// `live`) and, when it ends, takes the next one from the device work queue,
+// until no lane has one.  The lanes take their SSA steps and their leap
+// decisions in lockstep phases (up to ssa_budget SSA steps, then up to
+// dec_budget decisions) so that their instruction streams stay merged; a
+// lane in one phase waits while the others run the other.
 template <class N, int P, int SM>
-__device__ __forceinline__ void sweep(const N& net, const dev::Run& run, uint32_t lanes) {
-    const uint32_t lane = threadIdx.x & 31u;
-    if (lane >= lanes) return;
-    const uint32_t mask = lanes >= 32 ? 0xffffffffu : ((1u << lanes) - 1u);
+__device__ __forceinline__ void lockstep(const N& net, const dev::Run& run, uint32_t mask, State<P, SM>& s, Sim& st,
+                                         Out& o, bool live) {
     const size_t row_words = (size_t)net.ns() * (size_t)net.s_out();
-    State<P, SM> s;
-    Sim st;
-    Out o{nullptr, nullptr};
-    bool live = false, closed = false;
+    bool closed = false;
     for (;;) {
         if (!live && !closed) {
             const uint32_t sim = atomicAdd(run.queue, 1u);
@@ -592,6 +587,20 @@ __device__ __forceinline__ void sweep(const N& net, const dev::Run& run, uint32_
             live = false;
         }
     }
+}
+
+// Warp lockstep sweep: one thread per simulation, `lanes` simulations per
+// warp (lanes 0..lanes-1 of every warp work, the rest exit), simulations
+// pulled from the device work queue.
+template <class N, int P, int SM>
+__device__ __forceinline__ void sweep(const N& net, const dev::Run& run, uint32_t lanes) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if (lane >= lanes) return;
+    const uint32_t mask = lanes >= 32 ? 0xffffffffu : ((1u << lanes) - 1u);
+    State<P, SM> s;
+    Sim st;
+    Out o{nullptr, nullptr};
+    lockstep<N, P, SM>(net, run, mask, s, st, o, false);
 }
 
 // Words of one simulation's resumable state in the regrouping exchange:
@@ -683,8 +692,12 @@ __device__ __forceinline__ void get_state(const N& net, const uint32_t* xs, uint
 // each warp runs one phase only (with slots <= 32 in a 64-thread block, warp
 // 0 steps SSA while warp 1 decides).  Then SSA threads take up to ssa_budget
 // steps and deciding threads up to dec_budget decisions, and the block meets
-// at a barrier.  xs: dynamic shared memory of Packed<P, SM>::WORDS words
-// per thread.
+// at a barrier.  Once the work queue is closed and at most run.tail_sims
+// simulations are live in the block, they move to the first lanes of warp 0,
+// which finishes them in warp lockstep with no further barriers or state
+// exchange (a lone simulation steps about a third faster so) while the other
+// warps leave.  xs: dynamic shared memory of Packed<P, SM>::WORDS words per
+// thread.
 template <class N, int P, int SM>
 __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, uint32_t slots, uint32_t* xs) {
     __shared__ uint32_t s_cnt[2][32];
@@ -692,6 +705,9 @@ __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, 
     // [p][0] stepping warps after ssa_budget steps, [p][1] deciding warps
     // after their decisions.
     __shared__ uint32_t s_fin[2][2];
+    // set by a thread that found the work queue closed; read after a round's
+    // first barrier, written only after its second
+    __shared__ uint32_t s_closed;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t nt = blockDim.x, nw = nt >> 5;
     const uint32_t below = (1u << lane) - 1u;
@@ -700,11 +716,15 @@ __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, 
     Sim st;
     Out o{nullptr, nullptr};
     bool live = false;
+    if (tid == 0) s_closed = 0u;
+    __syncthreads();
     if (tid < slots) {
         const uint32_t sim = atomicAdd(run.queue, 1u);
         if (sim < run.n) {
             start_sim<N, P, SM>(net, run, s, st, sim);
             live = true;
+        } else {
+            s_closed = 1u;
         }
     }
     if (tid < 4) s_fin[tid >> 1][tid & 1] = 0u;
@@ -728,6 +748,21 @@ __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, 
             ndec += b;
         }
         if (nssa + ndec == 0u) break;  // the same counts in every thread
+        if (s_closed && nssa + ndec <= run.tail_sims && nssa + ndec <= 32u) {
+            // the tail: the live simulations to lanes 0..k-1, SSA ones first
+            if (live) {
+                const uint32_t pos = st.in_ssa ? offs + __popc(bs & below) : nssa + offd + __popc(bd & below);
+                put_state<P, SM>(xs, nt, pos, s, st);
+            }
+            __syncthreads();
+            const uint32_t k = nssa + ndec;
+            if (tid >= k) return;
+            get_state<N, P, SM>(net, xs, nt, tid, s, st);
+            all_props<N, P, SM>(net, s);
+            o = out_for(run, st.sim, row_words);
+            lockstep<N, P, SM>(net, run, k >= 32u ? 0xffffffffu : (1u << k) - 1u, s, st, o, true);
+            return;
+        }
         // the other parity's flags were last read in the round before this one
         if (tid < 2) s_fin[par ^ 1u][tid] = 0u;
         const uint32_t pad = (nssa + 31u) & ~31u;
@@ -791,6 +826,8 @@ __device__ __forceinline__ void sweep_rounds(const N& net, const dev::Run& run, 
             if (sim < run.n) {
                 start_sim<N, P, SM>(net, run, s, st, sim);
                 live = true;
+            } else {
+                s_closed = 1u;
             }
         }
     }

@@ -109,8 +109,9 @@ typedef struct {
                              256-thread blocks per SM (2: up to 128 registers per thread,
                              3: 80, 4: 64); 0 = library choice (autotuned, else 3 for
                              groups of 8+ lanes whose slots fit three blocks, else 2;
-                             2 for the register-resident sweep, whose kernel compiled for
-                             the network takes the budget given here) */
+                             1 for the register-resident sweep, whose kernel compiled for
+                             the network takes the budget given here; 1 is valid for that
+                             sweep only) */
     int32_t sched;        /* scheduling: 1 = block rounds regrouping simulations by phase
                              (the register-resident sweep moves their state through shared
                              memory), 2 = warp-local (no block barriers; warp lockstep);

@@ -178,7 +178,7 @@ def test_cli_usage_and_early_exit_codes(tmp_path):
     assert p.returncode == 256 - 4 and "do not fit" in p.stderr
 
 
-@pytest.mark.parametrize("kw", [{"min_blocks": 1}, {"min_blocks": 5}, {"ssa_steps": 0}, {"sched": 3},
+@pytest.mark.parametrize("kw", [{"min_blocks": -1}, {"min_blocks": 5}, {"ssa_steps": 0}, {"sched": 3},
                                 {"sched": -1}, {"warp_sims": 33}, {"warp_sims": -2},
                                 {"tiny_spec": 1}, {"tiny_spec": -2}])
 def test_run_cfg_rejected_before_any_device_work(kw):
