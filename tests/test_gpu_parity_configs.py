@@ -24,12 +24,14 @@ from tests.netutil import oracle_model, same_info
 
 pytestmark = pytest.mark.gpu
 
-PLAN_FIELDS = ("group", "threads", "min_blocks", "sched", "ssa_budget", "dec_budget")
+PLAN_FIELDS = ("group", "threads", "min_blocks", "sched", "ssa_budget", "dec_budget", "warp_sims")
 
 
 def _plan_cfg(model, n_plan, seed, uniform, **over):
     """The library's launch plan for a batch of n_plan simulations, pinned
-    as explicit settings (so a window of the batch runs the same plan)."""
+    as explicit settings (so a window of the batch runs the same plan).
+    warp_sims > 0 selects the register-resident sweep (tiny networks); 0
+    keeps the shared-memory sweep."""
     li = model.launch_info(n_plan, seed=seed, uniform_rates=uniform)
     kw = {f: getattr(li, f) for f in PLAN_FIELDS}
     kw.update(over)
@@ -91,7 +93,8 @@ def test_config1_schlogl_full_batch_every_simulation():
     compared (the slowest bistable simulations take about 14,000 steps)."""
     net = inputs.schlogl(4096)
     model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
-    _, kw = _plan_cfg(model, net.n, 1, 1)
+    li, kw = _plan_cfg(model, net.n, 1, 1)
+    assert li.warp_sims > 0, "Schlogl's plan is the register-resident sweep"
     out, info = _device(net, model, 0, net.n, 1, kw)
     o_out, o_info = oracle_model(net, seed=1).run(net.X0, np.asarray(net.c, np.float32))
     assert np.array_equal(out, o_out)
