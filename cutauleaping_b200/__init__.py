@@ -53,7 +53,7 @@ class RunCfg(C.Structure):
                 ("max_steps", C.c_uint32), ("sim_base", C.c_uint32), ("device", C.c_int32),
                 ("group", C.c_int32), ("threads", C.c_int32), ("uniform_rates", C.c_int32),
                 ("ssa_budget", C.c_int32), ("dec_budget", C.c_int32), ("min_blocks", C.c_int32),
-                ("sched", C.c_int32), ("warp_sims", C.c_int32), ("tiny_spec", C.c_int32)]
+                ("sched", C.c_int32), ("warp_sims", C.c_int32), ("spec", C.c_int32)]
 
 
 class ModelDims(C.Structure):
@@ -143,14 +143,14 @@ def _check(status: int, where: str):
 
 def run_cfg(*, seed=0, eps=0.03, nc=10, ssa_factor=10.0, ssa_steps=100, flags=0,
             max_steps=0xFFFFFFFF, sim_base=0, device=0, group=0, threads=0, uniform_rates=0,
-            ssa_budget=0, dec_budget=0, min_blocks=0, sched=0, warp_sims=0, tiny_spec=0) -> RunCfg:
+            ssa_budget=0, dec_budget=0, min_blocks=0, sched=0, warp_sims=0, spec=0) -> RunCfg:
     cfg = RunCfg()
     lib().ctl_run_cfg_default(C.byref(cfg))
     cfg.seed, cfg.eps, cfg.nc, cfg.ssa_factor = seed, eps, nc, ssa_factor
     cfg.ssa_steps, cfg.flags, cfg.max_steps, cfg.sim_base = ssa_steps, flags, max_steps, sim_base
     cfg.device, cfg.group, cfg.threads = device, group, threads
     cfg.uniform_rates, cfg.ssa_budget, cfg.dec_budget = uniform_rates, ssa_budget, dec_budget
-    cfg.min_blocks, cfg.sched, cfg.warp_sims, cfg.tiny_spec = min_blocks, sched, warp_sims, tiny_spec
+    cfg.min_blocks, cfg.sched, cfg.warp_sims, cfg.spec = min_blocks, sched, warp_sims, spec
     return cfg
 
 

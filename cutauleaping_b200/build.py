@@ -47,8 +47,10 @@ def _run(cmd, verbose):
 
 
 # Headers that the library also hands to NVRTC at run time, to compile
-# kernels specialised for one network (ctl_tiny.cu): embedded as strings.
-EMBEDDED = (("ctl_src_devmath", "ctl_devmath.cuh"), ("ctl_src_tiny_body", "ctl_tiny_body.cuh"))
+# kernels specialised for one network (ctl_tiny.cu, ctl_sweep.cu): embedded
+# as strings.
+EMBEDDED = (("ctl_src_devmath", "ctl_devmath.cuh"), ("ctl_src_tiny_body", "ctl_tiny_body.cuh"),
+            ("ctl_src_sweep_dev", "ctl_sweep_dev.cuh"))
 
 
 def _embed_sources(path: str) -> None:

@@ -25,6 +25,7 @@ typedef unsigned int uint32_t;
 typedef long long int64_t;
 typedef unsigned long long uint64_t;
 typedef unsigned long size_t;
+typedef unsigned long uintptr_t;
 #define FLT_MAX 3.402823466e+38F
 // The per-simulation record of include/ctl.h (same layout).
 typedef struct {

@@ -24,23 +24,41 @@
 //
 // Built with -fmad=false: no implicit FMA contraction; fma() is called
 // explicitly where it is meant.
+//
+// The device code is written against a model type M with the fields of
+// Model below.  The library's kernels read the network's geometry (species,
+// reactions, tree levels, sample counts) from that parameter block at run
+// time; a kernel compiled for one network at run time by NVRTC
+// (ctl_sweep.cu, sweep_spec_kernel) instantiates the same code with a type
+// whose geometry fields are static constexpr members of the same names, so
+// that loops over tree levels, species and samples have constant bounds and
+// every level's offsets fold into the code.  Both give the same bits.
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <cfloat>
 #include <cstdint>
-#include <cstring>
-#include <string>
 
 #include "ctl_internal.h"
+#endif
 #include "ctl_devmath.cuh"
+
+// Loops over the stored tree levels: unrolled when the geometry is a
+// compile-time constant (network-compiled kernels), left to the compiler
+// otherwise.
+#ifdef CTL_SPEC_GEOMETRY
+#define CTL_UNROLL_LEVELS _Pragma("unroll")
+#else
+#define CTL_UNROLL_LEVELS
+#endif
 
 namespace ctl {
 namespace dev {
 
-struct Model {
-    int S, R, P, logP, ns, s_out;
+// The model's tables in device memory (and the end time): the part of the
+// model that every kernel reads at run time.
+struct Tables {
     const uint32_t* __restrict__ reac_off;
     const uint32_t* __restrict__ reac_ent;
     const uint2* __restrict__ reac_desc;  // [R] packed reactants, x == 0xffffffff: general list
@@ -57,12 +75,21 @@ struct Model {
     const double* __restrict__ tvec;
     const uint32_t* __restrict__ cs;
     double tmax;
+};
+
+// Tables plus the geometry, read at run time (the library's own kernels).
+struct Model : Tables {
+    int S, R, P, logP, ns, s_out;
     // Stored levels of the binary sum tree: level 3, 6, 9, ... below the
     // root, and the root.  Stored level li holds the nodes that cover 2^shift
     // leaves; each is the pairwise sum of 2^d nodes of stored level li-1
     // (li = 0: of leaves).  Intermediate levels are recomputed in registers.
     int nlev;
-    int lev_shift[10], lev_d[10], lev_base[10], lev_count[10];
+    int lev_shift_v[10], lev_d_v[10], lev_base_v[10], lev_count_v[10];
+    __device__ __forceinline__ int lev_shift(int li) const { return lev_shift_v[li]; }
+    __device__ __forceinline__ int lev_d(int li) const { return lev_d_v[li]; }
+    __device__ __forceinline__ int lev_base(int li) const { return lev_base_v[li]; }
+    __device__ __forceinline__ int lev_count(int li) const { return lev_count_v[li]; }
 };
 
 // Shared-memory slot layout.  G == 1: element i of slot j at i*NS + j
@@ -205,7 +232,8 @@ __device__ __forceinline__ float react_factor(int32_t x, uint32_t st) {
 // 0.5 X (X-1) (coefficient 2) or the product of (X-e+1)/e (higher); zero when
 // a reactant count is below its coefficient.  Reactions with at most two
 // entries of coefficient <= 2 read one packed descriptor.
-__device__ __forceinline__ float prop(const Model& m, const Slot& sl, int r) {
+template <class M>
+__device__ __forceinline__ float prop(const M& m, const Slot& sl, int r) {
     float v = sl.cf(r);
     const uint2 d = m.reac_desc[r];
     if (d.x != 0xffffffffu) {
@@ -251,14 +279,16 @@ __device__ __forceinline__ double leafv(const Slot& sl, int r, int mode) {
 }
 
 // Node i of stored level li (li < 0: leaf i).
-__device__ __forceinline__ double tval(const Model& m, const Slot& sl, int li, int i, int mode) {
-    return li < 0 ? leafv(sl, i, mode) : sl.t(m.lev_base[li] + i);
+template <class M>
+__device__ __forceinline__ double tval(const M& m, const Slot& sl, int li, int i, int mode) {
+    return li < 0 ? leafv(sl, i, mode) : sl.t(m.lev_base(li) + i);
 }
 
 // Value of node i of stored level li: pairwise sum of its 2^d children.
 // ((c0+c1)+(c2+c3)) + ((c4+c5)+(c6+c7)) is exactly the binary-tree value.
-__device__ __forceinline__ double group_sum(const Model& m, const Slot& sl, int li, int i, int mode) {
-    const int d = m.lev_d[li], c0 = i << d, lc = li - 1;
+template <class M>
+__device__ __forceinline__ double group_sum(const M& m, const Slot& sl, int li, int i, int mode) {
+    const int d = m.lev_d(li), c0 = i << d, lc = li - 1;
     if (d == 1) return tval(m, sl, lc, c0, mode) + tval(m, sl, lc, c0 + 1, mode);
     if (d == 2)
         return (tval(m, sl, lc, c0, mode) + tval(m, sl, lc, c0 + 1, mode)) +
@@ -270,25 +300,29 @@ __device__ __forceinline__ double group_sum(const Model& m, const Slot& sl, int 
     return ((v0 + v1) + (v2 + v3)) + ((v4 + v5) + (v6 + v7));
 }
 
-__device__ __forceinline__ double tree_root(const Model& m, const Slot& sl) {
-    return sl.t(m.lev_base[m.nlev - 1]);
+template <class M>
+__device__ __forceinline__ double tree_root(const M& m, const Slot& sl) {
+    return sl.t(m.lev_base(m.nlev - 1));
 }
 
-template <int G>
-__device__ void build_tree(const Grp<G>& g, const Model& m, const Slot& sl, int mode) {
+template <int G, class M>
+__device__ void build_tree(const Grp<G>& g, const M& m, const Slot& sl, int mode) {
+    CTL_UNROLL_LEVELS
     for (int li = 0; li < m.nlev; li++) {
-        const int base = m.lev_base[li];
-        for (int i = (int)g.lane; i < m.lev_count[li]; i += G) sl.t(base + i) = group_sum(m, sl, li, i, mode);
+        const int base = m.lev_base(li);
+        for (int i = (int)g.lane; i < m.lev_count(li); i += G) sl.t(base + i) = group_sum(m, sl, li, i, mode);
         g.sync();
     }
 }
 
 // Leftmost leaf whose cumulative weight reaches x (ties go left); never a
 // zero leaf.  Same decisions as a level-by-level descent of the binary tree.
-__device__ __forceinline__ int descend(const Model& m, const Slot& sl, double x, int mode) {
+template <class M>
+__device__ __forceinline__ int descend(const M& m, const Slot& sl, double x, int mode) {
     int i = 0;
+    CTL_UNROLL_LEVELS
     for (int li = m.nlev - 1; li >= 0; li--) {
-        const int d = m.lev_d[li], c0 = i << d, lc = li - 1;
+        const int d = m.lev_d(li), c0 = i << d, lc = li - 1;
         int j;
         if (d == 1) {
             j = go_right(x, tval(m, sl, lc, c0, mode), tval(m, sl, lc, c0 + 1, mode)) ? 1 : 0;
@@ -314,8 +348,8 @@ __device__ __forceinline__ int descend(const Model& m, const Slot& sl, double x,
     return i;
 }
 
-template <int G>
-__device__ __forceinline__ void all_props(const Grp<G>& g, const Model& m, const Slot& sl) {
+template <int G, class M>
+__device__ __forceinline__ void all_props(const Grp<G>& g, const M& m, const Slot& sl) {
     for (int r = (int)g.lane; r < m.R; r += G) sl.pa(r) = prop(m, sl, r);
     g.sync();
     build_tree<G>(g, m, sl, 0);
@@ -324,8 +358,8 @@ __device__ __forceinline__ void all_props(const Grp<G>& g, const Model& m, const
 // After firing r: new propensities for the reactions that depend on the
 // changed species, then their tree paths (or a full rebuild when cheaper);
 // both give the same tree.
-template <int G>
-__device__ void update_after_fire(const Grp<G>& g, const Model& m, const Slot& sl, int r) {
+template <int G, class M>
+__device__ void update_after_fire(const Grp<G>& g, const M& m, const Slot& sl, int r) {
     const uint32_t d0 = m.dep_off[r], d1 = m.dep_off[r + 1];
     const uint32_t nd = d1 - d0;
     if (nd == 0) return;
@@ -334,12 +368,13 @@ __device__ void update_after_fire(const Grp<G>& g, const Model& m, const Slot& s
         sl.pa(rr) = prop(m, sl, rr);
     }
     g.sync();
-    if (nd >= (uint32_t)m.lev_count[0]) {  // touches about every bottom group: rebuild
+    if (nd >= (uint32_t)m.lev_count(0)) {  // touches about every bottom group: rebuild
         build_tree<G>(g, m, sl, 0);
         return;
     }
+    CTL_UNROLL_LEVELS
     for (int li = 0; li < m.nlev; li++) {
-        const int sh = m.lev_shift[li], base = m.lev_base[li];
+        const int sh = m.lev_shift(li), base = m.lev_base(li);
         int prev = -1;  // dependency lists are sorted: equal ancestors are adjacent
         for (uint32_t j = d0 + g.lane; j < d1; j += G) {
             const int i = (int)m.dep_ent[j] >> sh;
@@ -387,8 +422,8 @@ __device__ __forceinline__ Out out_of(const Run& run, uint32_t sim, size_t row_w
 
 // A0 == 0 (tau.cu:1665-1697, 2165-2196): the reference copies the last
 // recorded sample forward (writing the current state first if none exists).
-template <int G>
-__device__ void finish_zero(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl,
+template <int G, class M>
+__device__ void finish_zero(const Grp<G>& g, const M& m, const Run& run, const Slot& sl,
                             const Out& out, uint32_t& cursor) {
     const int so = m.s_out;
     const uint32_t ns = (uint32_t)m.ns;
@@ -420,8 +455,8 @@ struct Sim {
 
 constexpr int CONT = 0, DONE = 1;
 
-template <int G>
-__device__ void init_sim(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl, Sim& st,
+template <int G, class M>
+__device__ void init_sim(const Grp<G>& g, const M& m, const Run& run, const Slot& sl, Sim& st,
                          uint32_t sim) {
     const int S = m.S, R = m.R, P = m.P;
     g.sync();
@@ -446,8 +481,8 @@ __device__ void init_sim(const Grp<G>& g, const Model& m, const Run& run, const 
 
 // PreCalculations (tau.cu:1568-2093): the SSA hand-off decision and, unless
 // it hands off, one Cao tau-leap with critical reactions and rejection.
-template <int G>
-__device__ int decide_step(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl, Sim& st,
+template <int G, class M>
+__device__ int decide_step(const Grp<G>& g, const M& m, const Run& run, const Slot& sl, Sim& st,
                            const Out& out) {
     const int S = m.S, R = m.R, so = m.s_out;
     const uint32_t ns = (uint32_t)m.ns;
@@ -537,8 +572,10 @@ __device__ int decide_step(const Grp<G>& g, const Model& m, const Run& run, cons
         int mode = 1;
         if (!(fl & F_Q2_OFF) && !sl.cr(0)) {
             mode = 2;
-            if (lane == 0)  // the ancestors of leaf 0 are node 0 of every stored level
-                for (int li = 0; li < m.nlev; li++) sl.t(m.lev_base[li]) = group_sum(m, sl, li, 0, 2);
+            if (lane == 0) {  // the ancestors of leaf 0 are node 0 of every stored level
+                CTL_UNROLL_LEVELS
+                for (int li = 0; li < m.nlev; li++) sl.t(m.lev_base(li)) = group_sum(m, sl, li, 0, 2);
+            }
             g.sync();
         }
         pick = descend(m, sl, u53(wd.z, wd.w) * a0c, mode);
@@ -620,8 +657,8 @@ __device__ int decide_step(const Grp<G>& g, const Model& m, const Run& run, cons
 }
 
 // EventualSSASteps / LightweightSSA (tau.cu:2099-2454): one direct-method step.
-template <int G>
-__device__ int ssa_step(const Grp<G>& g, const Model& m, const Run& run, const Slot& sl, Sim& st,
+template <int G, class M>
+__device__ int ssa_step(const Grp<G>& g, const M& m, const Run& run, const Slot& sl, Sim& st,
                         const Out& out) {
     const int so = m.s_out;
     const uint32_t ns = (uint32_t)m.ns;
@@ -677,8 +714,8 @@ __device__ int ssa_step(const Grp<G>& g, const Model& m, const Run& run, const S
     return CONT;
 }
 
-template <int G>
-__device__ void finish_sim(const Grp<G>& g, const Model& m, const Run& run, const Sim& st, const Out& out) {
+template <int G, class M>
+__device__ void finish_sim(const Grp<G>& g, const M& m, const Run& run, const Sim& st, const Out& out) {
     const int so = m.s_out;
     if (out.samples)  // rows never reached read 0 (a sum gains nothing from them)
         for (uint32_t i = st.cursor; i < (uint32_t)m.ns; i++)
@@ -794,9 +831,10 @@ __device__ __forceinline__ Slot slot_of(unsigned char* smem, const Layout& lay, 
 // work.  The loop ends when the queue is drained and every slot is closed.
 // MINB selects the register budget: compiled so that MINB blocks of 256
 // threads can be resident per SM (2: up to 128 registers per thread, 3: 80,
-// 4: 64, spilling to local memory as needed).
-template <int G, int MINB>
-__global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layout lay) {
+// 4: 64, spilling to local memory as needed).  sweep_body is the kernel's
+// body for either model type; sweep_kernel is the library's kernel.
+template <int G, class M>
+__device__ __forceinline__ void sweep_body(const M& m, const Run& run, const Layout& lay) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t s_cnt[2];
     const int NS = (int)(blockDim.x / G);
@@ -947,6 +985,12 @@ __global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layo
     }
 }
 
+template <int G, int MINB>
+__global__ void __launch_bounds__(256, MINB) sweep_kernel(Model m, Run run, Layout lay) {
+    sweep_body<G>(m, run, lay);
+}
+
+#ifndef __CUDACC_RTC__
 // Host-side handle of the sweep kernel for G lanes per simulation in
 // register budget minb (2, 3 or 4 resident 256-thread blocks per SM).
 template <int G>
@@ -972,3 +1016,7 @@ const void* sweep_kernel_g128(int minb);
 const void* sweep_kernel_g256(int minb);
 
 }  // namespace ctl
+#else
+}  // namespace dev
+}  // namespace ctl
+#endif

@@ -136,10 +136,12 @@ const void* tiny_kernel_ptr(int P, int SM) {
 // Model-specialised kernels (NVRTC)
 // ---------------------------------------------------------------------------
 
-// The sources of ctl_devmath.cuh and ctl_tiny_body.cuh, embedded by the
-// build (cutauleaping_b200/build.py writes them into ctl_tiny_src.cpp).
+// The sources of ctl_devmath.cuh, ctl_tiny_body.cuh and ctl_sweep_dev.cuh,
+// embedded by the build (cutauleaping_b200/build.py writes them into
+// ctl_tiny_src.cpp).
 extern const char* const ctl_src_devmath;
 extern const char* const ctl_src_tiny_body;
+extern const char* const ctl_src_sweep_dev;
 
 namespace {
 
@@ -234,16 +236,18 @@ std::string spec_source(const HostTables& t, uint32_t flags, int minb, int sched
     return o.str();
 }
 
-const void* compile_spec(const std::string& src, std::string& why) {
+}  // namespace
+
+const void* nvrtc_kernel(const std::string& src, const char* name, std::string& why) {
     static Nvrtc nv = open_nvrtc();
     if (!nv.ok) {
         why = nv.why;
         return nullptr;
     }
-    const char* headers[] = {ctl_src_devmath, ctl_src_tiny_body};
-    const char* names[] = {"ctl_devmath.cuh", "ctl_tiny_body.cuh"};
+    const char* headers[] = {ctl_src_devmath, ctl_src_tiny_body, ctl_src_sweep_dev};
+    const char* names[] = {"ctl_devmath.cuh", "ctl_tiny_body.cuh", "ctl_sweep_dev.cuh"};
     nvrtcProgram prog;
-    if (nv.create(&prog, src.c_str(), "ctl_tiny_spec.cu", 2, headers, names) != NVRTC_SUCCESS) {
+    if (nv.create(&prog, src.c_str(), "ctl_spec.cu", 3, headers, names) != NVRTC_SUCCESS) {
         why = "nvrtcCreateProgram failed";
         return nullptr;
     }
@@ -275,15 +279,13 @@ const void* compile_spec(const std::string& src, std::string& why) {
         return nullptr;
     }
     cudaKernel_t k;
-    e = cudaLibraryGetKernel(&k, lib, "ctl_tiny_spec");
+    e = cudaLibraryGetKernel(&k, lib, name);
     if (e != cudaSuccess) {
         why = std::string("cudaLibraryGetKernel: ") + cudaGetErrorString(e);
         return nullptr;
     }
     return reinterpret_cast<const void*>(k);
 }
-
-}  // namespace
 
 const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, int minb, int sched, std::string* why) {
     const std::string src = spec_source(t, flags & dev::F_Q5_OFF, minb, sched);
@@ -294,7 +296,7 @@ const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, int minb, int 
             return e.kernel;
         }
     std::string w;
-    const void* k = compile_spec(src, w);
+    const void* k = nvrtc_kernel(src, "ctl_tiny_spec", w);
     g_spec.push_back({src, k, w});
     if (why) *why = w;
     return k;

@@ -58,4 +58,12 @@ struct SpecNet {
 // lock.
 const void* tiny_spec_kernel(const HostTables& t, uint32_t flags, int minb, int sched, std::string* why);
 
+// Compiles `src` for sm_100a with NVRTC (-fmad=false, the same arithmetic as
+// the library's kernels; the device headers ctl_devmath.cuh,
+// ctl_tiny_body.cuh and ctl_sweep_dev.cuh can be included), loads the CUBIN
+// and returns the kernel `name`, or nullptr with the reason in `why` when
+// NVRTC is missing or a step fails.  No caching and no lock: callers keep
+// their own cache.
+const void* nvrtc_kernel(const std::string& src, const char* name, std::string& why);
+
 }  // namespace ctl

@@ -123,9 +123,13 @@ typedef struct {
                              the live simulations per warp of a block on average); 0 =
                              library choice (used for such networks unless `group` is
                              set); -1 = never (shared-memory sweep)                    */
-    int32_t tiny_spec;    /* register-resident sweep: 0 = run a kernel compiled at run time for
-                             this network (NVRTC; the library's own kernel when NVRTC is
-                             absent), -1 = the library's own kernel                    */
+    int32_t spec;         /* kernels compiled at run time for this network (NVRTC, sm_100a;
+                             the library's own kernels when NVRTC is absent; same bits
+                             either way): 0 = library choice (register-resident sweep:
+                             always; shared-memory sweep: batches of at least 4,096
+                             simulations, where the seconds of compilation, once per
+                             process and network geometry, pay off), 1 = whenever
+                             possible, -1 = never                                    */
 } ctl_run_cfg;
 
 typedef struct {
@@ -143,7 +147,7 @@ typedef struct {
     int32_t ssa_budget, dec_budget;  /* work per simulation and round */
     int32_t warp_sims;    /* simulations per warp of the register-resident sweep, 0 when the
                              shared-memory sweep runs (ctl_run_cfg.warp_sims) */
-    int32_t specialized;  /* 1 when that sweep runs a kernel compiled for this network */
+    int32_t specialized;  /* 1 when the sweep runs a kernel compiled for this network  */
 } ctl_launch_info;
 
 /* ---- errors ------------------------------------------------------------ */

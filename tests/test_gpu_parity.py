@@ -98,7 +98,7 @@ def test_register_resident_sweep_bit_exact(name, net):
     m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
     li = m.launch_info(net.n)
     assert li.warp_sims > 0 and li.specialized == 1
-    assert m.launch_info(net.n, tiny_spec=-1).specialized == 0
+    assert m.launch_info(net.n, spec=-1).specialized == 0
     assert m.launch_info(net.n, group=4).warp_sims == 0
     # sched 2: warp lockstep; sched 1: block rounds regrouping the simulations by phase
     shapes = [(2, ws, th) for ws in (1, 3, 8, 32) for th in (32, 256)] + \
@@ -107,7 +107,7 @@ def test_register_resident_sweep_bit_exact(name, net):
         for sched, ws, threads in shapes:
             for sb, db in ((1, 1), (16, 2)):
                 out, info = m.run(net.X0, net.c, seed=61, warp_sims=ws, threads=threads, ssa_budget=sb,
-                                  dec_budget=db, sched=sched, tiny_spec=spec)
+                                  dec_budget=db, sched=sched, spec=spec)
                 what = f"{name} spec={spec} sched={sched} warp_sims={ws} threads={threads} ssa_budget={sb}"
                 assert np.array_equal(out, out_o), what
                 assert same_info(info, info_o) is None, what
@@ -124,7 +124,7 @@ def test_register_resident_quirk_switches(flags):
         m = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
         for spec in (0, -1):
             for sched in (1, 2):
-                out, info = m.run(net.X0, net.c, seed=8, flags=flags, warp_sims=4, tiny_spec=spec, sched=sched)
+                out, info = m.run(net.X0, net.c, seed=8, flags=flags, warp_sims=4, spec=spec, sched=sched)
                 assert np.array_equal(out, out_o), f"{name} flags={flags:#x} spec={spec} sched={sched}"
                 assert same_info(info, info_o) is None, f"{name} flags={flags:#x} spec={spec} sched={sched}"
 

@@ -104,18 +104,21 @@ def test_config1_schlogl_full_batch_every_simulation():
 
 def test_config2_full_batch_plan_and_graph():
     """64 x 128 synthetic network, the full 65,536-simulation batch at t_end 10
-    and 200 samples, on the library's plan for that batch, launched through a
-    captured CUDA graph (twice); 64 simulations spread over the batch are
-    compared with the oracle."""
+    and 200 samples, on the library's plan for that batch (the kernel
+    compiled for the network), launched through a captured CUDA graph
+    (twice); 64 simulations spread over the batch are compared with the
+    oracle, and a 512-simulation window run by the library's own kernel
+    with the graph's rows."""
     net = inputs.synthetic(64, 128, 65536, seed=0, t_end=10.0, samples=200)
     model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
     li, kw = _plan_cfg(model, net.n, 1, 1)
+    assert li.specialized == 1, "the full batch runs the kernel compiled for the network"
     out, info = _device(net, model, 0, net.n, 1, kw, graph=True)
     idx = np.linspace(0, net.n - 1, 64).astype(np.int64)
     o_info = _compare(net, out, info, 0, idx, 1, f"config 2 (G={li.group}, min_blocks={li.min_blocks})")
     assert o_info["steps"].min() > 20_000   # full-length trajectories
-    # the graph's results equal the plain device entry's on a window
-    out2, info2 = _device(net, model, 30000, 30512, 1, kw)
+    # the graph's results equal the library kernel's on a window
+    out2, info2 = _device(net, model, 30000, 30512, 1, dict(kw, spec=-1))
     assert np.array_equal(out2, out[30000:30512])
     assert same_info(info2, info[30000:30512]) is None
 
@@ -140,14 +143,14 @@ def test_config3_segments_with_perturbed_rates(sched):
 
 def test_config4_large_sparse_network_multiwarp_groups():
     """512 x 1024 sparse network at t_end 20 and 500 samples on the library's
-    plan for the full 16,384-simulation batch (whole warps per simulation):
-    a 1,184-simulation window, 16 of its simulations compared with the
-    oracle."""
+    plan for the full 16,384-simulation batch (whole warps per simulation, the
+    kernel compiled for the network): a 1,184-simulation window, 16 of its
+    simulations compared with the oracle."""
     net = inputs.synthetic(512, 1024, 16384, seed=0, t_end=20.0, samples=500, c_range=(1e-5, 1e-1),
                            x0_range=(1, 100000))
     model = ctl.Model.create(net.left, net.right, net.feed, net.tvec, net.cs)
-    li, kw = _plan_cfg(model, net.n, 1, 1)
-    assert li.group >= 64
+    li, kw = _plan_cfg(model, net.n, 1, 1, spec=1)  # the full batch's kernel, compiled for the network
+    assert li.group >= 64 and li.specialized == 1
     lo, hi = 9000, 9000 + 1184
     out, info = _device(net, model, lo, hi, 1, kw)
     idx = np.linspace(lo, hi - 1, 16).astype(np.int64)

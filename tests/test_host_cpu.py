@@ -180,7 +180,7 @@ def test_cli_usage_and_early_exit_codes(tmp_path):
 
 @pytest.mark.parametrize("kw", [{"min_blocks": -1}, {"min_blocks": 5}, {"ssa_steps": 0}, {"sched": 3},
                                 {"sched": -1}, {"warp_sims": 33}, {"warp_sims": -2},
-                                {"tiny_spec": 1}, {"tiny_spec": -2}])
+                                {"spec": 2}, {"spec": -2}])
 def test_run_cfg_rejected_before_any_device_work(kw):
     """Invalid run configurations fail with CTL_ERR_ARG in host code, before
     the library selects or touches a device."""
