@@ -141,6 +141,13 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to print its first row; a timed region
+            # shorter than that (config 1: 5 x 13 ms) would have no sample at
+            # all, so the region starts once the first row (taken under the
+            # warm-up steps' load) is in
+            t0 = time.time()
+            while not self.rows and self.proc.poll() is None and time.time() - t0 < 3.0:
+                time.sleep(0.005)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
