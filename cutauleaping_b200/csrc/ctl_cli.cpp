@@ -14,6 +14,8 @@
 //   CTL_SEED       Philox seed (default: time(NULL), like kernel.cu:176)
 //   CTL_FLAGS      quirk switches (ctl.h CTL_Q*_OFF), default 0
 //   CTL_EPS, CTL_NC, CTL_MAX_STEPS, CTL_GROUP, CTL_THREADS, CTL_WARP_SIMS
+//   CTL_SPEC       kernels compiled for the network at run time (ctl.h
+//                  ctl_run_cfg.spec): 0 library choice, 1 always, -1 never
 //   CTL_OUTPUT_EXISTING_OK=1  write into an existing output folder instead of
 //                  falling back to "./" (the reference falls back on any
 //                  mkdir failure, tau.cu:3133-3139)
@@ -196,6 +198,7 @@ static int run_cli(int argc, const char* argv[]) {
     cfg.group = (int32_t)env_u("CTL_GROUP", 0);
     cfg.threads = (int32_t)env_u("CTL_THREADS", 0);
     cfg.warp_sims = (int32_t)env_u("CTL_WARP_SIMS", 0);
+    cfg.spec = (int32_t)env_u("CTL_SPEC", 0);
     cfg.device = gpu;
     cfg.sim_base = offset;
     if (verbose) {
