@@ -43,7 +43,7 @@ EXPORTS = [
     "ctl_write_dynamics", "ctl_print_dynamics", "ctl_write_samples_binary", "ctl_write_run_report", "ctl_target_load", "ctl_target_free",
     "ctl_target_dims", "ctl_fitness", "ctl_fitness_device", "ctl_mlp_gemm", "ctl_mlp_nll_grad", "ctl_mlp_colsum",
     "ctl_mlp_adam", "ctl_mlp_pack_bytes", "ctl_mlp_pack", "ctl_mlp_screen", "ctl_mlp_wait_check", "ctl_run_device_sums",
-    "ctl_fitness_sums_device", "ctl_fitness_run",
+    "ctl_fitness_sums_device", "ctl_fitness_run", "ctl_spec_source",
 ]
 
 
@@ -110,6 +110,7 @@ def lib():
         L.ctl_run.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, P, P]
         L.ctl_run_device.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, P, P, P]
         L.ctl_launch_query.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, C.POINTER(LaunchInfo)]
+        L.ctl_spec_source.argtypes = [P, C.c_int32, C.c_int32, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
         L.ctl_run_device_noalloc.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, P, P, P]
         L.ctl_autotune.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, C.c_uint32, C.POINTER(LaunchInfo)]
         L.ctl_graph_create.argtypes = [P, C.POINTER(RunCfg), C.c_uint32, P, P, P, P, P, C.POINTER(P)]
@@ -224,6 +225,15 @@ class Model:
         _check(lib().ctl_run_device(self._h, C.byref(cfg), n, C.c_void_p(d_X0), C.c_void_p(d_c),
                                     C.c_void_p(d_out), C.c_void_p(d_info), C.c_void_p(stream)),
                "ctl_run_device")
+
+    def spec_source(self, group: int, min_blocks: int = 3) -> str:
+        """The CUDA source the library compiles with NVRTC for this network's
+        shared-memory sweep (ctl_spec_source); no device work."""
+        n = C.c_size_t()
+        _check(lib().ctl_spec_source(self._h, group, min_blocks, None, 0, C.byref(n)), "ctl_spec_source")
+        buf = C.create_string_buffer(n.value + 1)
+        _check(lib().ctl_spec_source(self._h, group, min_blocks, buf, n.value + 1, C.byref(n)), "ctl_spec_source")
+        return buf.value.decode()
 
     def launch_info(self, n, cfg: RunCfg | None = None, **kw) -> LaunchInfo:
         cfg = cfg if cfg is not None else run_cfg(**kw)

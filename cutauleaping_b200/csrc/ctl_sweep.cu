@@ -1116,6 +1116,29 @@ extern "C" ctl_status ctl_run(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, 
 // shared-memory sweep; then the per-round budgets -- and caches the fastest
 // for this (device, batch-size bucket, rate mode, flags).  Nothing slower
 // than the library's plan is cached.
+extern "C" ctl_status ctl_spec_source(const ctl_model* m, int32_t group, int32_t min_blocks, char* buf, size_t cap,
+                                      size_t* len) {
+    if (!m || !len || group < 1 || group > 256 || (group & (group - 1)) || min_blocks < 2 || min_blocks > 4) {
+        set_error("ctl_spec_source: group must be a power of two from 1 to 256 and min_blocks 2, 3 or 4");
+        return CTL_ERR_ARG;
+    }
+    try {
+        const std::string src = sweep_spec_source(m->t, std::min<int>(group, m->t.P), min_blocks);
+        *len = src.size();
+        if (!buf) return CTL_OK;
+        if (cap <= src.size()) {
+            set_error("ctl_spec_source: buffer too small");
+            return CTL_ERR_SHAPE;
+        }
+        std::memcpy(buf, src.data(), src.size());
+        buf[src.size()] = '\0';
+        return CTL_OK;
+    } catch (...) {
+        set_error("ctl_spec_source: out of host memory");
+        return CTL_ERR_OOM;
+    }
+}
+
 extern "C" ctl_status ctl_autotune(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n, const int32_t* d_X0,
                                    const float* d_c, uint32_t sample, ctl_launch_info* best) {
     if (!m || !d_X0 || !d_c || n == 0) return CTL_ERR_ARG;

@@ -195,6 +195,16 @@ ctl_status ctl_run_device(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
 ctl_status ctl_launch_query(ctl_model* m, const ctl_run_cfg* cfg, uint32_t n,
                             ctl_launch_info* li);
 
+/* Diagnostics (no counterpart in the reference; no device work): the CUDA
+ * source the library hands to NVRTC to compile the shared-memory sweep for
+ * this network with `group` lanes per simulation (capped at the tree's
+ * leaves) in register budget `min_blocks` (2, 3 or 4) -- see
+ * ctl_run_cfg.spec.  *len receives the source's length; with buf != NULL
+ * and cap > *len the source is copied there, NUL-terminated, else
+ * CTL_ERR_SHAPE (call again with a larger buffer). */
+ctl_status ctl_spec_source(const ctl_model* m, int32_t group, int32_t min_blocks, char* buf, size_t cap,
+                           size_t* len);
+
 /* The same sweep as ctl_run_device, for callers that cannot allocate device
  * memory (an application whose device memory comes only from its own pool,
  * a host that has fixed its device-memory budget, a layer that must not grow
