@@ -363,6 +363,29 @@ __device__ void update_after_fire(const Grp<G>& g, const M& m, const Slot& sl, i
     const uint32_t d0 = m.dep_off[r], d1 = m.dep_off[r + 1];
     const uint32_t nd = d1 - d0;
     if (nd == 0) return;
+    if (nd <= 2u * G) {
+        // at most two entries per lane: read them once and keep them in
+        // registers for the propensity pass and the tree levels (the same
+        // entries in the same order as the loops below)
+        const int e0 = g.lane < nd ? (int)m.dep_ent[d0 + g.lane] : -1;
+        const int e1 = g.lane + G < nd ? (int)m.dep_ent[d0 + g.lane + G] : -1;
+        if (e0 >= 0) sl.pa(e0) = prop(m, sl, e0);
+        if (e1 >= 0) sl.pa(e1) = prop(m, sl, e1);
+        g.sync();
+        if (nd >= (uint32_t)m.lev_count(0)) {
+            build_tree<G>(g, m, sl, 0);
+            return;
+        }
+        CTL_UNROLL_LEVELS
+        for (int li = 0; li < m.nlev; li++) {
+            const int sh = m.lev_shift(li), base = m.lev_base(li);
+            const int i0 = e0 >= 0 ? e0 >> sh : -1, i1 = e1 >= 0 ? e1 >> sh : -1;
+            if (i0 >= 0) sl.t(base + i0) = group_sum(m, sl, li, i0, 0);
+            if (i1 >= 0 && i1 != i0) sl.t(base + i1) = group_sum(m, sl, li, i1, 0);
+            g.sync();
+        }
+        return;
+    }
     for (uint32_t j = d0 + g.lane; j < d1; j += G) {
         int rr = (int)m.dep_ent[j];
         sl.pa(rr) = prop(m, sl, rr);
