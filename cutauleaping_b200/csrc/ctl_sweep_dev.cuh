@@ -363,10 +363,13 @@ __device__ void update_after_fire(const Grp<G>& g, const M& m, const Slot& sl, i
     const uint32_t d0 = m.dep_off[r], d1 = m.dep_off[r + 1];
     const uint32_t nd = d1 - d0;
     if (nd == 0) return;
-    if (nd <= 2u * G) {
+    if (G >= 8 && nd <= 2u * G) {
         // at most two entries per lane: read them once and keep them in
         // registers for the propensity pass and the tree levels (the same
-        // entries in the same order as the loops below)
+        // entries in the same order as the loops below).  One B200: 8 lanes
+        // on the 64 x 128 network 1,181 -> 1,123 ms per sweep; 4 lanes on
+        // the 32 x 64 network 6,620 -> 7,516 ms, so groups of fewer than 8
+        // lanes keep the loops.
         const int e0 = g.lane < nd ? (int)m.dep_ent[d0 + g.lane] : -1;
         const int e1 = g.lane + G < nd ? (int)m.dep_ent[d0 + g.lane + G] : -1;
         if (e0 >= 0) sl.pa(e0) = prop(m, sl, e0);
